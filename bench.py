@@ -1,0 +1,342 @@
+#!/usr/bin/env python3
+"""Benchmark: 10 keV primaries/s through transport + IRT + scoring on B200.
+
+A step is one pass of the hot path over one batch: 4096 primary electrons at
+10 keV in liquid water (box +-15 um, cutoff 7.5 eV, Philox key = seed), Phase A
++ B transport, rad_buf canonicalisation, IRT chemistry to 1 us, direct SSB
+scoring and DSB clustering on the 21x21 B-DNA fibre grid.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl native|reference]
+
+value    device time of K steps (CUDA events on the library's stream), inputs
+         resident in HBM; L2 is flushed (256 MB write) between steps, outside
+         the timed events.
+e2e      the same work through the public host API with pinned host buffers:
+         per-primary source energies uploaded, results / dose grid / rad_buf
+         read back every step (runAtEnergy's contract), IRT + scoring results
+         returned.
+N > 1    one process per GPU (torchrun); each rank runs its own 4096 primaries
+         (global ids rank*4096 + i, weak scaling); per-step summaries are
+         all-reduced with NCCL; timing is the max over ranks.
+--impl reference  times the CPU restatement of the reference's path (the
+         oracle; the WebGPU shaders / JS worker cannot run here) on all host
+         cores on a bounded sample per step.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [ROOT, os.path.join(ROOT, "webgpu-dna_b200")]
+
+METRIC = "10 keV primaries/s (transport+IRT+scoring)"
+UNIT = "primaries/s"
+NP = 4096
+E_EV = 10000.0
+WORKLOAD = ("4096 x 10 keV e- in liquid water, box +-15 um, cutoff 7.5 eV, Philox seed 0 -> "
+            "IRT to 1 us -> direct SSB + DSB on 21x21 B-DNA fibres")
+CPU_SAMPLE_PRIMARIES = 512
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "fallback": True}
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[0]) for r in self.rows if r and r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if len(r) > 1 and r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            for k, n in enumerate(names):
+                if len(r) > 4 + k and r[4 + k].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def cpu_reference_step(nthreads, sample, seed):
+    """One bounded sample of the path on the host cores (the oracle)."""
+    import numpy as np
+    import oracle
+    t0 = time.perf_counter()
+    o = oracle.transport(sample, E_EV, seed=seed, rng_mode=0, dna_enable=1, nthreads=nthreads)
+    nth = int((o["results"].view(np.uint32).reshape(-1, 8)[:, 5] == 0).sum())
+    oracle.irt(o["rad"], nth, E_EV, seed=seed, nthreads=nthreads)
+    oracle.score_direct(_odna(), o["rad"])
+    return time.perf_counter() - t0
+
+
+_ODNA = None
+
+
+def _odna():
+    global _ODNA
+    if _ODNA is None:
+        import oracle
+        _ODNA = oracle.DnaTarget()
+    return _ODNA
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    nthreads = os.cpu_count() or 1
+    sample = CPU_SAMPLE_PRIMARIES
+    for w in range(args.warmup):
+        cpu_reference_step(nthreads, max(32, sample // 8), 1000 + w)
+    dts = [cpu_reference_step(nthreads, sample, k) for k in range(args.steps)]
+    t = sum(dts)
+    value = sample * args.steps / t
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * t / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 transport / f64 IRT", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": WORKLOAD, "np": NP, "E_eV": E_EV,
+                       "sample": f"{sample} primaries per step through transport+IRT+scoring"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
+                             "sample": f"{sample} x 10 keV primaries per step, {args.steps} steps"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_native(args, ws, rank, local):
+    import ctypes as C
+    import numpy as np
+    import torch
+    import wgdna
+    from wgdna import _lib
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    L = _lib.lib()
+    ctx = wgdna.Context(max_primaries=NP, device=local)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream.cuda_stream)
+    dna = wgdna.build_dna_target()
+    p = wgdna.transport_params(NP, E_EV, 15000.0, 7.5, dna=dna, seed=args.seed, dna_enable=1)
+    p.pid_base = rank * NP
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    st = _lib.TransportStats()
+    ir = _lib.IrtResult()
+    ssb = _lib.SsbResult()
+    dsb = _lib.DsbResult()
+    summary = torch.zeros(64, dtype=torch.float64, device=dev)
+
+    def step_device():
+        _lib.check("wgdna_transport", L.wgdna_transport(ctx.h, C.byref(p), C.byref(st)))
+        _lib.check("wgdna_irt", L.wgdna_irt(ctx.h, st.n_therm, E_EV, args.seed + 1, C.byref(ir)))
+        _lib.check("wgdna_score", L.wgdna_score(ctx.h, 0x12345678, C.byref(ssb), C.byref(dsb)))
+        if ws > 1:
+            vals = [float(st.n_therm), float(st.dep_units), float(dsb.dsb), float(ssb.ssb)] + \
+                   [float(x) for x in np.array(ir.counts).reshape(-1)]
+            with torch.cuda.stream(stream):
+                summary[:len(vals)].copy_(torch.tensor(vals, dtype=torch.float64), non_blocking=True)
+                torch.distributed.all_reduce(summary)
+
+    # pinned host buffers for the end-to-end path
+    E_host = torch.full((NP,), E_EV, dtype=torch.float32, pin_memory=True)
+    res_h = torch.empty(NP * 8, dtype=torch.float32, pin_memory=True)
+    dose_h = torch.empty(ctx.vc ** 3, dtype=torch.int32, pin_memory=True)
+    rad_cap = 8_000_000
+    rad_h = torch.empty(rad_cap * 4, dtype=torch.float32, pin_memory=True)
+    p_e2e = wgdna.transport_params(NP, E_EV, 15000.0, 7.5, dna=dna, seed=args.seed, dna_enable=1)
+    p_e2e.pid_base = rank * NP
+    p_e2e.E_per_primary = E_host.data_ptr()
+    rad_n = C.c_uint64()
+    e2e_bytes = {"h2d": 0, "d2h": 0}
+
+    def step_e2e():
+        _lib.check("wgdna_run_transport",
+                   L.wgdna_run_transport(ctx.h, C.byref(p_e2e), C.c_void_p(res_h.data_ptr()),
+                                         C.c_void_p(dose_h.data_ptr()), C.c_void_p(rad_h.data_ptr()), rad_cap,
+                                         C.byref(rad_n), C.byref(st)))
+        _lib.check("wgdna_irt", L.wgdna_irt(ctx.h, st.n_therm, E_EV, args.seed + 1, C.byref(ir)))
+        _lib.check("wgdna_score", L.wgdna_score(ctx.h, 0x12345678, C.byref(ssb), C.byref(dsb)))
+        e2e_bytes["h2d"] = NP * 4 + C.sizeof(p_e2e)
+        e2e_bytes["d2h"] = (NP * 32 + ctx.vc ** 3 * 4 + min(rad_n.value, rad_cap) * 16 + C.sizeof(st) +
+                            C.sizeof(ir) + C.sizeof(ssb) + C.sizeof(dsb))
+
+    for _ in range(args.warmup):
+        step_device()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t_tr, t_irt, t_canon, t_sc = [], [], [], []
+    launches = 0
+    with Clocks(local) as clk:
+        barrier()
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(k))
+                ev[k][0].record(stream)
+            step_device()
+            with torch.cuda.stream(stream):
+                ev[k][1].record(stream)
+            t_tr.append(st.ms_transport)
+            t_canon.append(st.ms_canon)
+            t_irt.append(ir.ms)
+            t_sc.append(ssb.ms + dsb.ms)
+            launches += 13
+        barrier()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    tot_ms = sum(ms)
+    if ws > 1:
+        t = torch.tensor([tot_ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        tot_ms = float(t.item())
+    value = ws * NP * args.steps / (tot_ms / 1000.0)
+
+    # end-to-end through the public host API
+    for _ in range(2):
+        step_e2e()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step_e2e()
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    if ws > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = ws * NP * args.steps / e2e_s
+
+    # roofline of the dominant kernel: algorithmic bytes per launch / its mean duration
+    pk = peaks()
+    mean = lambda a: sum(a) / len(a)
+    stages = {"irt": mean(t_irt), "transport": mean(t_tr), "canon": mean(t_canon), "scoring": mean(t_sc)}
+    dom = max(stages, key=stages.get)
+    R, S = st.rad_n_stored, st.sec_n
+    if dom == "transport":
+        alg = 16 * R + 8 * R + 96 * S + 32 * NP + 4 * st.steps / 50.0
+    elif dom == "irt":
+        alg = 16 * R + 34 * R + 16 * ir.n_events
+    else:
+        alg = 16 * R
+    achieved = alg / (stages[dom] / 1000.0) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf)).get(dom)
+        except Exception:
+            traffic = None
+    clocks = clk.summary()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 transport / f64 IRT", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "np_per_gpu": NP, "E_eV": E_EV, "seed": args.seed,
+                       "l2": "256 MB write between timed steps (outside the events)",
+                       "parallelism": f"primary shards x{ws}"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": e2e_bytes["h2d"],
+                    "d2h_bytes_per_step": e2e_bytes["d2h"]},
+            "gpu_launches": launches,
+            "stage_ms": {k: round(v, 4) for k, v in stages.items()},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk["hbm_gbs"],
+                         "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
+                         "peak_source": "fallback" if pk.get("fallback") else "measured"},
+            "clocks": clocks,
+            "work": {"rad_n": int(R), "sec_n": int(S), "steps": int(st.steps), "irt_pairs": int(ir.n_pairs),
+                     "irt_events": int(ir.n_events), "ssb": int(ssb.ssb), "dsb": int(dsb.dsb)},
+        }
+        if ws == 1 and not args.no_cpu:
+            nthreads = os.cpu_count() or 1
+            cpu_reference_step(nthreads, 64, 99)
+            dt = cpu_reference_step(nthreads, CPU_SAMPLE_PRIMARIES, 7)
+            line["cpu_baseline"] = {"value": CPU_SAMPLE_PRIMARIES / dt, "unit": UNIT, "cores": nthreads,
+                                    "kind": "port",
+                                    "sample": f"{CPU_SAMPLE_PRIMARIES} x 10 keV primaries through "
+                                              f"transport+IRT+scoring (oracle, {nthreads} threads)"}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["native", "reference"], default="native")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    ws, rank, local = dist_init(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank)
+        else:
+            run_native(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

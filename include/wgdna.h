@@ -1,0 +1,161 @@
+/* wgdna.h -- C ABI of the B200 path for allaunthefox/webgpu-dna's hot path:
+ * electron transport in liquid water -> Karamitros 9-reaction IRT chemistry ->
+ * SSB/DSB scoring on the 21x21 B-DNA fibre grid.
+ *
+ * Plain C types only (no CUDA or torch types).  Every function returns an int
+ * status (WGDNA_OK = 0, negative on error) and wgdna_last_error() describes the
+ * last error of the calling thread.  A context owns one CUDA stream and the
+ * device buffers of one call at a time; it is not thread-safe.  Host buffers
+ * are caller-owned.  Buffer overflows are not errors: they are counted in the
+ * *_dropped fields, as the reference counts sec_dropped / rad_dropped
+ * (src/gpu/dispatch.ts:124-126,190-192).  Device-side bounded waits that give
+ * up set device_error and make the call return WGDNA_ERR_DEVICE.
+ */
+#ifndef WGDNA_H
+#define WGDNA_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WGDNA_OK 0
+#define WGDNA_ERR_ARG (-1)
+#define WGDNA_ERR_CUDA (-2)
+#define WGDNA_ERR_TABLES (-3)
+#define WGDNA_ERR_CAPACITY (-4)
+#define WGDNA_ERR_DEVICE (-5)
+#define WGDNA_ERR_NOMEM (-6)
+#define WGDNA_ERR_STATE (-7)
+
+typedef struct wgdna_ctx wgdna_ctx;
+
+/* Context configuration.  Replaces initGPU + allocateBuffers
+ * (src/gpu/device.ts:11-33, src/gpu/buffers.ts:48-85): the buffer caps are the
+ * reference's MAX_SEC / MAX_RAD / VC (src/physics/constants.ts:51-60). */
+typedef struct {
+    int device;                 /* CUDA device ordinal */
+    const char *tables_path;    /* cross_sections.bin; NULL = next to the library */
+    uint32_t max_primaries;     /* largest np per call */
+    uint32_t max_sec;           /* MAX_SEC (5,000,000) */
+    uint64_t max_rad;           /* MAX_RAD (16,000,000) */
+    uint32_t vc;                /* dose grid edge VC (128) */
+    uint32_t reserved;
+} wgdna_cfg;
+
+void wgdna_default_cfg(wgdna_cfg *cfg);
+int wgdna_create(const wgdna_cfg *cfg, wgdna_ctx **out);      /* ensurePipelines, app.ts:65-84 */
+void wgdna_destroy(wgdna_ctx *ctx);
+const char *wgdna_last_error(void);
+int wgdna_version(void);
+/* Run the context's work on a caller's cudaStream_t (NULL = the context's own). */
+int wgdna_set_stream(wgdna_ctx *ctx, void *cuda_stream);
+
+/* ---------------------------------------------------------------- Phase A+B */
+/* The uniform structs P (src/gpu/dispatch.ts:13-42) and SP (dispatch.ts:45-70). */
+typedef struct {
+    uint32_t np;                /* P.n */
+    float E_eV;                 /* P.be */
+    float box_nm;               /* P.box (half width) */
+    float ce_eV;                /* P.ce */
+    uint32_t max_steps;         /* P.ms (65536) */
+    uint32_t sec_steps;         /* MAX_SEC_STEPS (2000), constants.ts:66 */
+    float start_half;           /* P.start_half */
+    uint32_t dna_enable;        /* P.dna_enable */
+    uint32_t dna_grid_n;
+    float dna_rise, dna_spacing, dna_x0, dna_r_bb;
+    uint32_t pid_base;          /* global id of primary 0 (sharding); w = (pid_base+i)*8 + code */
+    uint64_t seed;              /* Philox key */
+    const float *E_per_primary; /* optional host array of np energies (eV); NULL = E_eV for all */
+} wgdna_transport_params;
+
+typedef struct {
+    uint32_t counters[8];       /* primary.wgsl:24-35: OH, eaq, H, H3O+, DNA hits, H2, sec idx, rad idx */
+    uint32_t sec_stats[8];      /* [1] cutoff, [2] bounds, [3] steps, [4] tertiary ions */
+    uint32_t dbg[8];            /* [0] ions, [1] exc, [2] escaped, [3] primaries, [4] sum W*10 */
+    uint64_t rad_n_raw, rad_n_stored, rad_dropped;
+    uint64_t sec_n_raw, sec_n, sec_dropped;
+    uint64_t dep_units;         /* sum of the dose grid (100 units per eV) */
+    double dep_eV_f64;          /* every deposit summed in f64 */
+    uint64_t steps;             /* electron steps */
+    float ms_transport;         /* CUDA-event time of the transport kernel */
+    float ms_canon;             /* CUDA-event time of rad_buf canonicalisation */
+    uint32_t device_error;
+    uint32_t n_therm;           /* primaries that did not escape */
+} wgdna_transport_stats;
+
+/* Phase A + Phase B (dispatch.ts:106-145) into device memory of the context.
+ * rad_buf is left in canonical order: grouped by primary, the primary's own
+ * entries first, then each secondary's, each in emission order. */
+int wgdna_transport(wgdna_ctx *ctx, const wgdna_transport_params *p, wgdna_transport_stats *st);
+/* Readbacks of the last transport (dispatch.ts:148-240).  Any pointer may be
+ * NULL.  results: np*8 words (R struct, primary.wgsl:9); dose: vc^3 u32;
+ * rad: 4 floats per entry, at most rad_cap entries. */
+int wgdna_transport_copy_out(wgdna_ctx *ctx, float *results, uint32_t *dose, float *rad,
+                             uint64_t rad_cap, uint64_t *rad_n);
+/* Both of the above in one call: the device part of runAtEnergy (dispatch.ts:85-240). */
+int wgdna_run_transport(wgdna_ctx *ctx, const wgdna_transport_params *p, float *results,
+                        uint32_t *dose, float *rad, uint64_t rad_cap, uint64_t *rad_n,
+                        wgdna_transport_stats *st);
+
+/* ---------------------------------------------------------------- Phase C */
+typedef struct {
+    double counts[7][5];        /* alive OH, eaq, H, H2O2(+prod), H2 at 1,10,100 ps,1,10,100 ns,1 us */
+    double G[7][5];             /* per 100 eV of n_therm * E_eV (irt-worker.js:670-682) */
+    uint64_t rxn_counts[9];     /* irt-worker.js:685-694 order */
+    uint64_t n_reacted, n_tracks, n_pairs, n_events;
+    uint64_t chem_n;
+    float ms;
+    uint32_t device_error;
+} wgdna_irt_result;
+
+/* runChemistryWorker (src/chemistry/worker.ts:32-87, public/irt-worker.js:370-699)
+ * on a host rad_buf (4 floats per entry, w = pid*8 + species code). */
+int wgdna_run_irt(wgdna_ctx *ctx, const float *rad_buf, uint64_t rad_n, uint32_t n_therm,
+                  double E_eV, uint64_t seed, wgdna_irt_result *out);
+/* The same on the rad_buf left in device memory by the last wgdna_transport. */
+int wgdna_irt(wgdna_ctx *ctx, uint32_t n_therm, double E_eV, uint64_t seed, wgdna_irt_result *out);
+
+/* ---------------------------------------------------------------- scoring */
+typedef struct {
+    uint32_t grid_N, n_bp_per, n_fibers, n_bp;
+    double rise, r_bb, spacing_nm, x0, L_nm;
+} wgdna_dna_info;
+
+/* buildDNATarget (src/physics/dna-geometry.ts:16-68), host only.  Array
+ * pointers may be NULL; sizes: fy/fz grid_N^2, rbb0/rbb1 2*n_bp_per floats. */
+int wgdna_build_dna_target(double L_nm, uint32_t grid_N, double spacing_nm, float *fy, float *fz,
+                           float *rbb0, float *rbb1, wgdna_dna_info *info);
+/* Upload the target used by the scoring entry points (default 3000 nm, 21, 150 nm). */
+int wgdna_set_dna_target(wgdna_ctx *ctx, double L_nm, uint32_t grid_N, double spacing_nm);
+
+typedef struct {
+    uint64_t ssb, ssb0, ssb1, candidates, in_reach;
+    uint32_t lcg_state;         /* makeSsbRng state after the pass */
+    float ms;
+} wgdna_ssb_result;
+
+typedef struct {
+    uint64_t dsb, ssb0, ssb1;
+    double dsb_expected;
+    float ms;
+} wgdna_dsb_result;
+
+/* scoreDirectSSB_events (src/scoring/ssb-dsb.ts:135-217).  hits (2*n_bp bytes)
+ * is read and OR-ed into when not NULL, like the Uint8Array the reference
+ * combines later (combineHits, ssb-dsb.ts:413-418). */
+int wgdna_score_direct(wgdna_ctx *ctx, const float *rad, uint64_t rad_n, uint32_t lcg_state,
+                       uint8_t *hits, wgdna_ssb_result *out);
+/* scoreIndirectSSB (ssb-dsb.ts:43-121). */
+int wgdna_score_indirect(wgdna_ctx *ctx, const float *pos, const uint32_t *alive, uint64_t n,
+                         uint32_t lcg_state, uint8_t *hits, wgdna_ssb_result *out);
+/* clusterDSB (ssb-dsb.ts:348-407). */
+int wgdna_cluster_dsb(wgdna_ctx *ctx, const uint8_t *hits, wgdna_dsb_result *out);
+/* Direct SSB + DSB clustering of the rad_buf left by the last wgdna_transport
+ * (app.ts:182-185 with the worker backend, where indirect scoring is skipped). */
+int wgdna_score(wgdna_ctx *ctx, uint32_t lcg_state, wgdna_ssb_result *ssb, wgdna_dsb_result *dsb);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -31,7 +31,7 @@ class TransportParams(C.Structure):
                 ("dna_enable", C.c_uint32), ("dna_grid_n", C.c_uint32),
                 ("dna_rise", C.c_float), ("dna_spacing", C.c_float), ("dna_x0", C.c_float),
                 ("dna_r_bb", C.c_float), ("sec_steps", C.c_uint32), ("rng_mode", C.c_uint32),
-                ("seed", C.c_uint64)]
+                ("seed", C.c_uint64), ("pid_base", C.c_uint32), ("E_per_primary", C.c_void_p)]
 
 
 class TransportOut(C.Structure):
@@ -109,7 +109,7 @@ def dna_x0(L_nm=3000.0, rise=0.34):
 
 def transport(np_, E_eV, seed=0, box_nm=15000.0, ce_eV=7.5, dna_enable=None, rng_mode=0,
               max_sec=5_000_000, max_rad=16_000_000, sec_steps=2000, max_steps=65536,
-              start_half=0.0, vc=128, nthreads=None, want_dose=True):
+              start_half=0.0, vc=128, nthreads=None, want_dose=True, pid_base=0, E_per_primary=None):
     """Phase A + B on the CPU.  Returns a dict of numpy arrays and counters.
 
     rng_mode 0 = Philox streams (bit-exact with the CUDA path), 1 = the
@@ -120,7 +120,11 @@ def transport(np_, E_eV, seed=0, box_nm=15000.0, ce_eV=7.5, dna_enable=None, rng
     p = TransportParams(np_, box_nm, ce_eV, max_steps, E_eV, max_sec, vc, max_rad, start_half,
                         dna_enable, DNA_DEFAULT["grid_n"], DNA_DEFAULT["rise"],
                         DNA_DEFAULT["spacing"], float(dna_x0()), DNA_DEFAULT["r_bb"],
-                        sec_steps, rng_mode, seed)
+                        sec_steps, rng_mode, seed, pid_base, None)
+    if E_per_primary is not None:
+        E_arr = np.ascontiguousarray(E_per_primary, dtype=np.float32)
+        assert E_arr.size == np_
+        p.E_per_primary = E_arr.ctypes.data
     res = np.zeros(np_ * 8, dtype=np.float32)
     dose = np.zeros(vc ** 3, dtype=np.uint32) if want_dose else None
     o = TransportOut()

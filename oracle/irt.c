@@ -18,8 +18,11 @@
  *        load draws of particle k      counter (blk, k, pid, 2)
  *        acceptance draw of pair i<j   counter (j>>2, i, pid, 3), word j&3
  *        SamplePDC trial t of (i,j)    counter (i, j, pid, 4 | t<<4)
- *        Brownian sync of (idx,jj)     counter (idx, jj, pid, 5 | b<<4), b=0..2
- *        acceptance draw of (idx,jj)   counter (idx, jj, pid, 5 | 3<<4), word 0
+ *        product idx, partner jj       counter (idx, jj, pid, 5): words 0-2 are
+ *                                      the Box-Muller radius draws of x, y, z,
+ *                                      word 3 the acceptance draw; counter
+ *                                      (idx, jj, pid, 5 | 1<<4): words 0-2 are
+ *                                      the Box-Muller angle draws
  *      A 53-bit double is made from two words, a 32-bit one as (w+0.5)/2^32.
  *   2. Events with equal times leave the heap in (t, i, j) order (the
  *      reference's binary heap leaves ties in an arbitrary order).
@@ -385,12 +388,13 @@ static void run_track(const float *rad, const uint64_t *idx, uint32_t n, uint32_
                 double Dj = IRT_D[s2];
                 double dt = ev.t - w->tb[jj];
                 double xj = w->px[jj], yj = w->py[jj], zj = w->pz[jj];
+                om_u4 q0 = om_philox(id, jj, pid, 5u, g.k0, g.k1);
                 if (dt > 0) {
                     double sig = sqrt(2.0 * Dj * dt);
+                    om_u4 q1 = om_philox(id, jj, pid, 5u | (1u << 4), g.k0, g.k1);
                     double nrm[3];
                     for (int b = 0; b < 3; ++b) {
-                        om_u4 q = om_philox(id, jj, pid, 5u | ((uint32_t)b << 4), g.k0, g.k1);
-                        double u1 = om_u01d(q.v[0], q.v[1]), u2 = om_u01d(q.v[2], q.v[3]);
+                        double u1 = om_u01d32(q0.v[b]), u2 = om_u01d32(q1.v[b]);
                         nrm[b] = sqrt(-2 * om_log(u1 + 1e-30)) * om_cos(6.2831853 * u2);
                     }
                     xj += nrm[0] * sig; yj += nrm[1] * sig; zj += nrm[2] * sig;
@@ -400,8 +404,7 @@ static void run_track(const float *rad, const uint64_t *idx, uint32_t n, uint32_
                 if (r2 > C.r_cut2) continue;
                 acc->pairs++;
                 double r0 = sqrt(r2);
-                om_u4 q = om_philox(id, jj, pid, 5u | (3u << 4), g.k0, g.k1);
-                double U = om_u01d32(q.v[0]);
+                double U = om_u01d32(q0.v[3]);
                 double t = sample_irt(&g, id, jj, r0, r2i, Di + Dj, U);
                 if (t >= 0) {
                     double ta = ev.t + t;

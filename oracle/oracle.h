@@ -40,6 +40,8 @@ typedef struct {
     uint32_t sec_steps;     /* MAX_SEC_STEPS (2000), constants.ts:66 */
     uint32_t rng_mode;      /* 0 = Philox (build), 1 = reference xoshiro */
     uint64_t seed;          /* Philox key (mode 0) / floor(E) seed (mode 1) */
+    uint32_t pid_base;      /* global id of primary 0 */
+    const float *E_per_primary;  /* optional per-primary energy (NULL: E_eV) */
 } orc_transport_params;
 
 typedef struct {

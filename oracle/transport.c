@@ -239,7 +239,7 @@ static void put(emit_t *e, float x, float y, float z, float code) {
     }
     float *d = s->rad + 4 * s->n;
     d[0] = x; d[1] = y; d[2] = z; d[3] = code + e->pidf;
-    s->key[s->n] = ((uint64_t)e->pid << 34) | ((uint64_t)e->sub << 17) | e->seq;
+    s->key[s->n] = ((uint64_t)(e->pid - e->p->pid_base) << 34) | ((uint64_t)e->sub << 17) | e->seq;
     e->seq++;
     s->n++;
 }
@@ -610,11 +610,12 @@ static void run_secondary(emit_t *e, sec_t *q) {                  /* secondary.w
 }
 
 static void run_primary(const orc_transport_params *p, uint32_t idx, sink_t *sk, float *res) {
-    emit_t e = {p, sk, idx, 0, 0, (float)idx * 8.0f};
+    uint32_t gid = p->pid_base + idx;
+    emit_t e = {p, sk, gid, 0, 0, (float)gid * 8.0f};
     rng_t s;
-    if (p->rng_mode == 1) rng_reference(&s, idx, (uint32_t)p->seed);
-    else rng_philox(&s, p->seed, idx, 0);
-    float E = p->E_eV;
+    if (p->rng_mode == 1) rng_reference(&s, gid, (uint32_t)p->seed);
+    else rng_philox(&s, p->seed, gid, 0);
+    float E = p->E_per_primary ? p->E_per_primary[idx] : p->E_eV;
     float px = 0.0f, py = 0.0f, pz = 0.0f;
     float sh = p->start_half;
     if (sh > 0.0f) {

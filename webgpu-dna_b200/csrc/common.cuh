@@ -1,0 +1,87 @@
+// common.cuh -- shared definitions of the CUDA path (device structs, errors).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+
+#include "../../include/wgdna.h"
+
+namespace wg {
+
+// Error bits raised on the device (read back after each stage).
+enum : uint32_t {
+    DERR_QUEUE_WAIT = 1u << 0,     // a bounded wait for a queued secondary gave up
+    DERR_IDLE_WAIT = 1u << 1,      // a warp waited too long for work / termination
+    DERR_KEY_RANGE = 1u << 2,      // secondary index or sequence overflowed the key
+    DERR_TRACK_SIZE = 1u << 3,     // a track exceeded the per-block capacity
+    DERR_HEAP = 1u << 4,           // IRT event storage overflow
+    DERR_SEG_SORT = 1u << 5,       // a rad_buf segment exceeded the sort capacity
+};
+
+// Cross-section tables (public/cross_sections.wgsl:9-72) in device memory.
+struct Tables {
+    // small tables, copied to shared memory by the transport kernel, in this order
+    const float* small;            // see SMALL_* offsets
+    const float* xwc;              // 5 x (N_WE*N_WR) Born CDF
+    const float* xwt;              // 5 x (N_WE*N_WR) Born energy transfer
+    float log_xe0, inv_log_xe_step, log_xae0, inv_log_xae_step;
+    uint32_t xn, n_ae, n_ac, n_we, n_wr, n_vib;
+};
+
+// offsets inside Tables::small (floats)
+constexpr int XN_ = 100, NAE_ = 25, NAC_ = 25, NWE_ = 58, NWR_ = 250, NVIB_ = 38;
+constexpr int S_XE = 0;
+constexpr int S_XI = S_XE + XN_;
+constexpr int S_XC = S_XI + XN_;
+constexpr int S_XL = S_XC + XN_;
+constexpr int S_XSF = S_XL + XN_;          // 5 x 100
+constexpr int S_XEF = S_XSF + 5 * XN_;     // 5 x 100
+constexpr int S_XAE = S_XEF + 5 * XN_;
+constexpr int S_XAC = S_XAE + NAE_;        // 625
+constexpr int S_XWE = S_XAC + NAE_ * NAC_;
+constexpr int S_XVE = S_XWE + NWE_;
+constexpr int S_XVS = S_XVE + NVIB_;
+constexpr int S_XVMF = S_XVS + NVIB_;      // 38 x 9
+constexpr int S_VIB = S_XVMF + NVIB_ * 9;  // 9
+constexpr int S_TOTAL = S_VIB + 9;
+constexpr int S_TOTAL_PAD = (S_TOTAL + 3) & ~3;
+
+// Global state of one transport run (device memory, zeroed before the run).
+struct DevState {
+    uint32_t counters[8];      // primary.wgsl:24-35 semantics
+    uint32_t sec_stats[8];     // secondary.wgsl sec_stats
+    uint32_t dbg[8];           // primary.wgsl dbg (dbg[2] = escaped count)
+    unsigned long long rad_next;   // rad_buf slots reserved (may exceed capacity)
+    unsigned long long rad_drop;   // rad_buf entries dropped at capacity
+    unsigned long long steps;      // electron steps taken
+    double dep_f64;                // every deposit, f64
+    uint32_t sec_tail;             // secondaries reserved
+    uint32_t sec_head;             // secondaries taken
+    uint32_t sec_drop;             // secondaries dropped at capacity
+    uint32_t prim_next;            // primaries taken
+    int live;                      // particles started and not finished
+    uint32_t err;
+    uint32_t pad[2];
+};
+
+// One queued secondary (the Particle struct of primary.wgsl:14, with the
+// primary id and emission index instead of the RNG state).
+struct __align__(16) SecRec {
+    float4 pe;        // x, y, z, E
+    float4 dir;       // dx, dy, dz, (unused)
+    uint4 meta;       // pid, sub, epoch (ready flag), 0
+};
+
+}  // namespace wg
+
+#define WG_CUDA_OK(expr)                                                     \
+    do {                                                                     \
+        cudaError_t e_ = (expr);                                             \
+        if (e_ != cudaSuccess) {                                             \
+            wg_set_error("%s:%d %s: %s", __FILE__, __LINE__, #expr,          \
+                         cudaGetErrorString(e_));                            \
+            return WGDNA_ERR_CUDA;                                           \
+        }                                                                    \
+    } while (0)
+
+void wg_set_error(const char* fmt, ...);

@@ -1,0 +1,505 @@
+// irt.cu -- Karamitros 2011 9-reaction IRT radiolysis chemistry to 1 us.
+//
+// Follows public/irt-worker.js of allaunthefox/webgpu-dna (species and
+// reaction tables :191-286, sampleIRT :116-184 with SamplePDC :91-113, erfcinv
+// :31-39, erfcx :53-88, the per-primary event loop :470-667 and pairWithAlive
+// :430-465).  The reference runs the primaries one after another on one CPU
+// thread; here one warp owns one track (primary) at a time and the warps of a
+// persistent grid pull tracks from a counter:
+//
+// * load: entries of the track (codes 4/7 skipped, 7 counted as initial H2)
+//   are displaced in f64 with the thermalisation Gaussians, 32 at a time;
+// * initial pairing: tiles of 32 particles held in lane registers, the partner
+//   j broadcast to all lanes; one Philox block gives the acceptance draws of
+//   four consecutive partners;
+// * events: a binary heap ordered by (t, i, j), kept by lane 0; the
+//   product re-pairing (pairWithAlive) is spread over the 32 lanes.
+//
+// Random draws are keyed by what they are for (track, particle, pair), so the
+// result does not depend on scheduling; the CPU oracle uses the same streams:
+//   load of particle k            philox(blk, k, pid, 2), 53-bit doubles
+//   acceptance of pair i<j         philox(j>>2, i, pid, 3), word j&3
+//   SamplePDC trial t of (i, j)    philox(i, j, pid, 4 | t<<4)
+//   product idx, partner jj        philox(idx, jj, pid, 5): Box-Muller radii
+//                                  x,y,z + acceptance; philox(.., 5 | 1<<4):
+//                                  Box-Muller angles.
+#include "irt.cuh"
+#include "dmath.cuh"
+
+namespace wg {
+
+
+__constant__ IrtConst c_irt;
+
+
+constexpr int IB = 128;                  // threads per block (4 warps)
+
+__device__ __forceinline__ double erfcinv_(double x) {                       // :31-39
+    if (x <= 0 || x >= 2) return 0;
+    double p = x > 1 ? 2 - x : x;
+    double t = sqrt(-2 * log_(p / 2));
+    double y = t - (2.515517 + 0.802853 * t + 0.010328 * t * t) /
+                   (1 + 1.432788 * t + 0.189269 * t * t + 0.001308 * t * t * t);
+    y *= 0.7071067811865475;
+    return x > 1 ? -y : y;
+}
+
+__constant__ double c_erfcx[28] = {
+    -1.3026537197817094, 6.4196979235649026e-1, 1.9476473204185836e-2, -9.561514786808631e-3,
+    -9.46595344482036e-4, 3.66839497852761e-4, 4.2523324806907e-5, -2.0278578112534e-5,
+    -1.624290004647e-6, 1.303655835580e-6, 1.5626441722e-8, -8.5238095915e-8,
+    6.529054439e-9, 5.059343495e-9, -9.91364156e-10, -2.27365122e-10,
+    9.6467911e-11, 2.394038e-12, -6.886027e-12, 8.94487e-13,
+    3.13092e-13, -1.12708e-13, 3.81e-16, 7.106e-15,
+    -1.523e-15, -9.4e-17, 1.21e-16, -2.8e-17};
+
+__device__ double erfcx_pos(double x) {                                      // :53-88, x >= 0
+    if (x >= 6) {
+        double f = 0;
+        for (int n = 30; n >= 1; --n) f = (0.5 * n) / (x + f);
+        return 0.5641895835477563 / (x + f);
+    }
+    double t = 2.0 / (2.0 + x);
+    double ty = 4 * t - 2;
+    double d = 0, dd = 0;
+    for (int j = 27; j > 0; --j) { double tmp = d; d = ty * d - dd + c_erfcx[j]; dd = tmp; }
+    return t * exp_(0.5 * (c_erfcx[0] + ty * d) - dd);
+}
+__device__ __forceinline__ double erfcx_(double x) {
+    if (x < 0) return 2 * exp_(x * x) - erfcx_pos(-x);
+    return erfcx_pos(x);
+}
+
+__device__ __noinline__ double sample_pdc(uint32_t i, uint32_t j, uint32_t pid, uint32_t k0, uint32_t k1,
+                                          double a, double b) {                // :91-113
+    double p = 2.0 * sqrt(2.0 * b / a);
+    double q = 2.0 / sqrt(2.0 * b / a);
+    double M = fmax(1.0 / (a * a), 3.0 * b / a);
+    for (uint32_t trial = 0; trial < 10000; ++trial) {
+        u4 w = philox(i, j, pid, 4u | (trial << 4), k0, k1);
+        double U = u01d(w.x, w.y);
+        double X;
+        if (U < p / (p + q * M)) { double h = U * (p + q * M) / 2; X = h * h; }
+        else { double h = 2 / ((1 - U) * (p + q * M) / M); X = h * h; }
+        U = u01d(w.z, w.w);
+        double sqX = sqrt(X);
+        double lambdax = exp_(-b * b / X) * (1.0 - a * sqrt(3.141592653589793 * X) * erfcx_(b / sqX + a * sqX));
+        if ((X <= 2.0 * b / a && U <= lambdax) || (X >= 2.0 * b / a && U * M / X <= lambdax)) return X;
+    }
+    return -1.0;
+}
+
+// sampleIRT (:116-184) with the acceptance draw U supplied
+__device__ __forceinline__ double sample_irt(const IrtConst& C, uint32_t i, uint32_t j, uint32_t pid,
+                                             uint32_t k0, uint32_t k1, double r0, int ri, double D, double U) {
+    if (C.type[ri] == 0) {
+        double sigma = C.sigma[ri], rc = C.rc[ri];
+        if (sigma <= 0 || D <= 0) return -1;
+        if (r0 <= sigma) return 0;
+        double r0e = r0;
+        if (rc != 0) r0e = -rc / (1 - exp_(rc / r0));
+        if (r0e <= sigma) return 0;
+        double Winf = sigma / r0e;
+        if (U <= 0 || U >= Winf) return -1;
+        double ei = erfcinv_(r0e * U / sigma);
+        if (fabs(ei) < 1e-10) return -1;
+        double dr = r0e - sigma;
+        return 0.25 * dr * dr / (D * ei * ei);
+    }
+    double sigma_c = C.sigma[ri], rc = C.rc[ri];
+    double a = C.a_pdc[ri], b, sc_chk = sigma_c, r0_chk = r0;
+    if (rc == 0) {
+        b = (r0 - sigma_c) / 2;
+    } else {
+        double coth_r0 = 1.0 + 2.0 / expm1_(2.0 * (rc / (2 * r0)));
+        b = rc / 4 * (coth_r0 - C.coth_sig[ri]);
+        r0_chk = -rc / (1 - exp_(rc / r0));
+        sc_chk = C.sigma_eff[ri];
+    }
+    if (sc_chk > r0_chk) return (C.prob[ri] > U) ? 0 : -1;
+    double Winf = sc_chk / r0_chk * C.kobs[ri] / C.kdif[ri];
+    if (Winf > U) {
+        double X = sample_pdc(i, j, pid, k0, k1, a, b);
+        if (X > 0) return X / D;
+    }
+    return -1;
+}
+
+// lane-0 binary heap on (t, a, b)
+__device__ __forceinline__ bool ev_less(double t1, int2 x, double t2, int2 y) {
+    if (t1 != t2) return t1 < t2;
+    if (x.x != y.x) return x.x < y.x;
+    return x.y < y.y;
+}
+__device__ void heap_sift_down(double* T, int2* AB, uint32_t n, uint32_t p) {
+    double tp = T[p];
+    int2 ap = AB[p];
+    for (;;) {
+        uint32_t l = 2 * p + 1;
+        if (l >= n) break;
+        uint32_t s = l;
+        double ts = T[l];
+        int2 as = AB[l];
+        if (l + 1 < n) {
+            double tr = T[l + 1];
+            int2 ar = AB[l + 1];
+            if (ev_less(tr, ar, ts, as)) { s = l + 1; ts = tr; as = ar; }
+        }
+        if (!ev_less(ts, as, tp, ap)) break;
+        T[p] = ts; AB[p] = as;
+        p = s;
+    }
+    T[p] = tp; AB[p] = ap;
+}
+__device__ void heap_push(double* T, int2* AB, uint32_t& n, double t, int2 ab) {
+    uint32_t c = n++;
+    while (c > 0) {
+        uint32_t p = (c - 1) >> 1;
+        if (!ev_less(t, ab, T[p], AB[p])) break;
+        T[c] = T[p]; AB[c] = AB[p];
+        c = p;
+    }
+    T[c] = t; AB[c] = ab;
+}
+
+__global__ void __launch_bounds__(IB) k_irt(IArgs A) {
+    __shared__ double s_tl[IB / 32][35];
+    __shared__ IrtConst s_c;
+    for (int k = threadIdx.x; k < (int)(sizeof(IrtConst) / 4); k += IB)
+        reinterpret_cast<uint32_t*>(&s_c)[k] = reinterpret_cast<const uint32_t*>(&c_irt)[k];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const uint32_t gw = blockIdx.x * (IB / 32) + wl;
+    const IrtConst& C = s_c;
+    for (int k = lane; k < 35; k += 32) s_tl[wl][k] = 0.0;
+    double* px = A.px + (size_t)gw * A.cap;
+    double* py = A.py + (size_t)gw * A.cap;
+    double* pz = A.pz + (size_t)gw * A.cap;
+    double* tb = A.tb + (size_t)gw * A.cap;
+    int8_t* sp = A.sp + (size_t)gw * A.cap;
+    uint8_t* alive = A.alive + (size_t)gw * A.cap;
+    double* HT = A.ev_t + (size_t)gw * A.ecap;
+    int2* HAB = A.ev_ab + (size_t)gw * A.ecap;
+    unsigned long long rxn[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    unsigned long long n_reacted = 0, n_pairs = 0, n_events = 0, n_tracks = 0;
+    const double CP[7] = {0.001, 0.01, 0.1, 1, 10, 100, 1000};
+
+    for (;;) {
+        uint32_t p = 0;
+        if (lane == 0) p = atomicAdd(A.track_next, 1u);
+        p = __shfl_sync(0xffffffffu, p, 0);
+        if (p >= A.nseg) break;
+        unsigned long long s = A.seg_off[p], e = A.seg_off[p + 1];
+        if (s == e) continue;
+        const uint32_t pid = A.pid_base + p;
+        // ---------------------------------------------------------- load (:475-537)
+        uint32_t n = 0, h2 = 0;
+        bool overflow = false;
+        for (unsigned long long c = s; c < e; c += 32) {
+            unsigned long long idx = c + lane;
+            bool valid = idx < e;
+            int code = -1;
+            float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (valid) { r = A.rad[idx]; code = (int)rintf(r.w) % 8; }
+            bool keep = valid && code >= 0 && code != 4 && code != 7;
+            h2 += __popc(__ballot_sync(0xffffffffu, valid && code == 7));
+            unsigned m = __ballot_sync(0xffffffffu, keep);
+            uint32_t k = n + __popc(m & lt);
+            if (keep && k < A.cap) {
+                double x = r.x, y = r.y, z = r.z;
+                int spc = code;
+                double sigma = 0;
+                int disp = 0;
+                uint32_t blk = 0, wi = 4;
+                u4 wb = {0, 0, 0, 0};
+                auto nextd = [&]() -> double {
+                    if (wi == 4) { wb = philox(blk++, k, pid, 2u, A.k0, A.k1); wi = 0; }
+                    uint32_t a_ = wi == 0 ? wb.x : wb.z;
+                    uint32_t b_ = wi == 0 ? wb.y : wb.w;
+                    wi += 2;
+                    return u01d(a_, b_);
+                };
+                if (code == 5) spc = 1;
+                else if (code == 0 || code == 3) { if (nextd() < 0.5) { disp = 1; sigma = C.sig_oh; } }
+                else if (code == 1) { disp = 1; sigma = C.sig_eaq; }
+                else if (code == 2) { disp = 1; sigma = C.sig_h; }
+                else if (code == 6) spc = 5;
+                if (disp) {
+                    double c6[3];
+                    for (int ax = 0; ax < 3; ++ax) {
+                        double r1 = nextd(), r2 = nextd(), r3 = nextd(), r4 = nextd(), r5 = nextd(), r6 = nextd();
+                        c6[ax] = (r1 + r2 + r3 + r4 + r5 + r6 - 3) * 1.4142135623730951;
+                    }
+                    x += sigma * c6[0]; y += sigma * c6[1]; z += sigma * c6[2];
+                }
+                px[k] = x; py[k] = y; pz[k] = z; tb[k] = 0.0;
+                sp[k] = (int8_t)spc; alive[k] = 1;
+            }
+            if (keep && k >= A.cap) overflow = true;
+            n += __popc(m);
+        }
+        if (__any_sync(0xffffffffu, overflow)) { if (lane == 0) atomicOr(A.err, DERR_TRACK_SIZE); continue; }
+        if (n == 0) continue;
+        n_tracks++;
+        __syncwarp();
+        __threadfence_block();
+        // alive counts per species (lane 0 keeps them)
+        uint32_t cnt[6] = {0, 0, 0, 0, 0, 0};
+        for (uint32_t c = 0; c < n; c += 32) {
+            uint32_t k = c + lane;
+            int spc = k < n ? sp[k] : -1;
+            for (int q = 0; q < 6; ++q) cnt[q] += __popc(__ballot_sync(0xffffffffu, spc == q));
+        }
+        // -------------------------------------------------- initial pairing (:539-558)
+        uint32_t nev = 0;
+        bool ev_over = false;
+        for (uint32_t i0 = 0; i0 < n; i0 += 32) {
+            uint32_t i = i0 + lane;
+            bool hi = i < n;
+            double xi = 0, yi = 0, zi = 0, Di = 0;
+            int si = 0;
+            if (hi) { xi = px[i]; yi = py[i]; zi = pz[i]; si = sp[i]; Di = C.D[si]; }
+            uint32_t row = 0;                      // reaction index of (si, s) in 4-bit fields, 15 = none
+            for (int q = 5; q >= 0; --q) row = (row << 4) | (uint32_t)(C.map[si * 6 + q] & 15);
+            uint32_t cblk = 0xffffffffu;
+            u4 cw = {0, 0, 0, 0};
+            for (uint32_t j = i0 + 1; j < n; ++j) {
+                bool acc = false;
+                double t = 0;
+                if (hi && j > i) {
+                    int sj = sp[j];
+                    int ri = (int)((row >> (4 * sj)) & 15u);
+                    if (ri != 15) {
+                        double dx = xi - px[j], dy = yi - py[j], dz = zi - pz[j];
+                        double r2 = dx * dx + dy * dy + dz * dz;
+                        if (r2 <= C.r_cut2) {
+                            n_pairs++;
+                            double r0 = sqrt(r2);
+                            if ((j >> 2) != cblk) { cblk = j >> 2; cw = philox(cblk, i, pid, 3u, A.k0, A.k1); }
+                            uint32_t wd = (j & 3) == 0 ? cw.x : (j & 3) == 1 ? cw.y : (j & 3) == 2 ? cw.z : cw.w;
+                            double U = u01d32(wd);
+                            t = sample_irt(C, i, j, pid, A.k0, A.k1, r0, ri, Di + C.D[sj], U);
+                            acc = (t >= 0 && t < 1000);
+                        }
+                    }
+                }
+                unsigned m = __ballot_sync(0xffffffffu, acc);
+                if (m) {
+                    uint32_t slot = nev + __popc(m & lt);
+                    if (acc) {
+                        if (slot < A.ecap) { HT[slot] = t; HAB[slot] = make_int2((int)i, (int)j); }
+                        else ev_over = true;
+                    }
+                    nev += __popc(m);
+                }
+            }
+        }
+        if (__any_sync(0xffffffffu, ev_over)) { if (lane == 0) atomicOr(A.err, DERR_HEAP); continue; }
+        __syncwarp();
+        __threadfence_block();
+        // ------------------------------------------------------- event loop (:566-660)
+        uint32_t hn = nev;
+        if (lane == 0) for (int k = (int)hn / 2 - 1; k >= 0; --k) heap_sift_down(HT, HAB, hn, (uint32_t)k);
+        uint32_t ntot = n;
+        double h2c = (double)h2;
+        int cp = 0;
+        bool heap_over = false;
+        for (;;) {
+            hn = __shfl_sync(0xffffffffu, hn, 0);
+            if (hn == 0) break;
+            double et = 0;
+            int ei = 0, ej = 0;
+            if (lane == 0) {
+                et = HT[0]; int2 ab = HAB[0];
+                ei = ab.x; ej = ab.y;
+                hn--;
+                if (hn > 0) { HT[0] = HT[hn]; HAB[0] = HAB[hn]; heap_sift_down(HT, HAB, hn, 0); }
+                n_events++;
+                while (cp < 7 && et >= CP[cp]) {
+                    s_tl[wl][cp * 5 + 0] += cnt[0]; s_tl[wl][cp * 5 + 1] += cnt[1];
+                    s_tl[wl][cp * 5 + 2] += cnt[2]; s_tl[wl][cp * 5 + 3] += cnt[4];
+                    s_tl[wl][cp * 5 + 4] += h2c;
+                    cp++;
+                }
+            }
+            et = __shfl_sync(0xffffffffu, et, 0);
+            ei = __shfl_sync(0xffffffffu, ei, 0);
+            ej = __shfl_sync(0xffffffffu, ej, 0);
+            int valid = 0, si = 0, sj = 0, ri = -1;
+            if (lane == 0) {
+                if (alive[ei] && alive[ej]) {
+                    si = sp[ei]; sj = sp[ej];
+                    ri = C.map[(si < sj ? si : sj) * 6 + (si < sj ? sj : si)];
+                    if (ri >= 0) {
+                        valid = 1;
+                        alive[ei] = 0; alive[ej] = 0;
+                        cnt[si]--; cnt[sj]--;
+                        n_reacted++;
+                        rxn[ri]++;
+                        if (ri == 3 || ri == 4 || ri == 6) h2c += 1;
+                    }
+                }
+            }
+            valid = __shfl_sync(0xffffffffu, valid, 0);
+            if (!valid) continue;
+            si = __shfl_sync(0xffffffffu, si, 0);
+            sj = __shfl_sync(0xffffffffu, sj, 0);
+            ri = __shfl_sync(0xffffffffu, ri, 0);
+            int np_ = C.nprod[ri];
+            if (np_ == 0) continue;
+            double sqDi = sqrt(C.D[si]), sqDj = sqrt(C.D[sj]);
+            double ww = sqDi + sqDj;
+            double xa = px[ei], ya = py[ei], za = pz[ei];
+            double xb = px[ej], yb = py[ej], zb = pz[ej];
+            double mx = (sqDj * xa + sqDi * xb) / ww;
+            double my = (sqDj * ya + sqDi * yb) / ww;
+            double mz = (sqDj * za + sqDi * zb) / ww;
+            for (int pp = 0; pp < np_; ++pp) {
+                int nsp = pp == 0 ? C.prod0[ri] : C.prod1[ri];
+                uint32_t id = ntot;
+                if (id >= A.cap) break;
+                double nx, ny, nz;
+                if (np_ == 1) { nx = mx; ny = my; nz = mz; }
+                else if (pp == 0) { nx = xa; ny = ya; nz = za; }
+                else { nx = xb; ny = yb; nz = zb; }
+                if (lane == 0) {
+                    px[id] = nx; py[id] = ny; pz[id] = nz; tb[id] = et;
+                    sp[id] = (int8_t)nsp; alive[id] = 1;
+                    cnt[nsp]++;
+                }
+                ntot++;
+                __syncwarp();
+                __threadfence_block();
+                // pairWithAlive (:430-465)
+                double Di = C.D[nsp];
+                for (uint32_t c0 = 0; c0 < ntot; c0 += 32) {
+                    uint32_t jj = c0 + lane;
+                    bool acc = false;
+                    double ta = 0;
+                    if (jj < ntot && jj != id && alive[jj]) {
+                        int s2 = sp[jj];
+                        int r2i = C.map[nsp * 6 + s2];
+                        if (r2i >= 0) {
+                            double Dj = C.D[s2];
+                            double dt = et - tb[jj];
+                            double xj = px[jj], yj = py[jj], zj = pz[jj];
+                            u4 q0 = philox(id, jj, pid, 5u, A.k0, A.k1);
+                            if (dt > 0) {
+                                double sig = sqrt(2.0 * Dj * dt);
+                                u4 q1 = philox(id, jj, pid, 5u | (1u << 4), A.k0, A.k1);
+                                double g0 = sqrt(-2 * log_(u01d32(q0.x) + 1e-30)) * cos_(6.2831853 * u01d32(q1.x));
+                                double g1 = sqrt(-2 * log_(u01d32(q0.y) + 1e-30)) * cos_(6.2831853 * u01d32(q1.y));
+                                double g2 = sqrt(-2 * log_(u01d32(q0.z) + 1e-30)) * cos_(6.2831853 * u01d32(q1.z));
+                                xj += g0 * sig; yj += g1 * sig; zj += g2 * sig;
+                            }
+                            double dx = nx - xj, dy = ny - yj, dz = nz - zj;
+                            double r2 = dx * dx + dy * dy + dz * dz;
+                            if (r2 <= C.r_cut2) {
+                                n_pairs++;
+                                double r0 = sqrt(r2);
+                                double U = u01d32(q0.w);
+                                double t = sample_irt(C, id, jj, pid, A.k0, A.k1, r0, r2i, Di + Dj, U);
+                                if (t >= 0) { ta = et + t; acc = ta < 1000; }
+                            }
+                        }
+                    }
+                    unsigned m = __ballot_sync(0xffffffffu, acc);
+                    while (m) {
+                        int src = __ffs(m) - 1;
+                        m &= m - 1;
+                        double tt = __shfl_sync(0xffffffffu, ta, src);
+                        uint32_t pj = __shfl_sync(0xffffffffu, jj, src);
+                        if (lane == 0) {
+                            if (hn < A.ecap) {
+                                int a = (int)(pj < id ? pj : id), bq = (int)(pj < id ? id : pj);
+                                heap_push(HT, HAB, hn, tt, make_int2(a, bq));
+                            } else heap_over = true;
+                        }
+                    }
+                }
+                __syncwarp();
+                __threadfence_block();
+            }
+        }
+        if (lane == 0) {
+            if (heap_over) atomicOr(A.err, DERR_HEAP);
+            while (cp < 7) {
+                s_tl[wl][cp * 5 + 0] += cnt[0]; s_tl[wl][cp * 5 + 1] += cnt[1];
+                s_tl[wl][cp * 5 + 2] += cnt[2]; s_tl[wl][cp * 5 + 3] += cnt[4];
+                s_tl[wl][cp * 5 + 4] += h2c;
+                cp++;
+            }
+        }
+        __syncwarp();
+    }
+    // per-warp totals -> global
+    for (int k = 0; k < 9; ++k) {
+        unsigned long long v = rxn[k];
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0 && v) atomicAdd(&A.acc[k], v);
+    }
+    unsigned long long vals[4] = {n_reacted, n_pairs, n_events, n_tracks};
+    for (int k = 0; k < 4; ++k) {
+        unsigned long long v = vals[k];
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0 && v) atomicAdd(&A.acc[9 + k], v);
+    }
+    __syncwarp();
+    for (int k = lane; k < 35; k += 32)
+        if (s_tl[wl][k] != 0.0) atomicAdd(&A.acc_tl[k], s_tl[wl][k]);
+}
+
+// codes -> grouping keys (pid << 34 | original index) for a caller's rad_buf
+__global__ void k_group_keys(const float4* rad, unsigned long long n, unsigned long long* key, uint32_t* maxpid) {
+    unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+    uint32_t mp = 0;
+    if (i < n) {
+        int w = (int)rintf(rad[i].w);
+        uint32_t pid = w >= 0 ? (uint32_t)(w / 8) : 0u;
+        key[i] = ((unsigned long long)pid << 34) | i;
+        mp = pid;
+    }
+    for (int o = 16; o; o >>= 1) mp = max(mp, __shfl_xor_sync(0xffffffffu, mp, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(maxpid, mp);
+}
+
+// longest segment
+__global__ void k_seg_max(const unsigned long long* off, uint32_t nseg, unsigned long long* out) {
+    unsigned long long m = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nseg; i += gridDim.x * blockDim.x)
+        m = max(m, off[i + 1] - off[i]);
+    for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+// ------------------------------------------------------------------ host side
+cudaError_t irt_set_constants(const IrtConst& c) { return cudaMemcpyToSymbol(c_irt, &c, sizeof c); }
+
+int irt_blocks(int device) {
+    int sms = 0, per = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_irt, IB, 0);
+    if (per < 1) per = 1;
+    return sms * per;
+}
+
+cudaError_t launch_irt(const IArgs& a, int blocks, cudaStream_t s) {
+    k_irt<<<blocks, IB, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_group_keys(const float4* rad, unsigned long long n, unsigned long long* key, uint32_t* maxpid,
+                              cudaStream_t s) {
+    cudaMemsetAsync(maxpid, 0, 4, s);
+    if (n) k_group_keys<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(rad, n, key, maxpid);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_seg_max(const unsigned long long* off, uint32_t nseg, unsigned long long* out, cudaStream_t s) {
+    cudaMemsetAsync(out, 0, 8, s);
+    k_seg_max<<<148, 256, 0, s>>>(off, nseg, out);
+    return cudaGetLastError();
+}
+
+}  // namespace wg

@@ -1,0 +1,49 @@
+"""Phase C: Karamitros 9-reaction IRT (src/chemistry/worker.ts:32-87 +
+public/irt-worker.js:370-699), run by the CUDA kernel through the C ABI."""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .constants import CHECKPOINT_LABELS, CHECKPOINTS_NS, IRT_WORKER_RXN_LABELS
+
+
+def _chem_result(r, rad_n, log=None):
+    timeline = []
+    for c in range(7):
+        g = r.G[c]
+        timeline.append({"label": CHECKPOINT_LABELS[c], "t_ns": CHECKPOINTS_NS[c], "G_OH": g[0], "G_eaq": g[1],
+                         "G_H": g[2], "G_H2O2": g[3], "G_H2": g[4]})
+    rxn_info = [{"label": IRT_WORKER_RXN_LABELS[k], "count": int(r.rxn_counts[k])} for k in range(9)]
+    res = {"chem_n": int(rad_n), "t_wall": float(r.ms), "timeline": timeline, "chem_pos_final": None,
+           "chem_alive_final": None, "n_reacted": int(r.n_reacted), "rxn_info": rxn_info,
+           "n_tracks": int(r.n_tracks), "n_pairs": int(r.n_pairs), "n_events": int(r.n_events),
+           "counts": np.array(r.counts, dtype=np.float64)}
+    if log:
+        for cp in timeline:
+            log(f"  {cp['label']} {cp['G_OH']:.3f} {cp['G_eaq']:.3f} {cp['G_H']:.3f} "
+                f"{cp['G_H2O2']:.3f} {cp['G_H2']:.3f}", "data")
+        log(f"  IRT kernel: {res['n_reacted']} reactions in {res['t_wall'] / 1000:.3f}s ({rad_n} radicals)", "data")
+    return res
+
+
+def run_chemistry_worker(ctx, rad_buf, rad_n, n_therm, E_eV, log=None, seed=1):
+    """runChemistryWorker: IRT on a host rad_buf (vec4 f32, w = pid*8 + code).
+
+    Like the reference worker, chem_pos_final / chem_alive_final are None, so
+    indirect SSB scoring is skipped downstream (app.ts:178-180)."""
+    rad = np.ascontiguousarray(np.asarray(rad_buf, dtype=np.float32).reshape(-1)[: 4 * int(rad_n)])
+    r = _lib.IrtResult()
+    _lib.check("wgdna_run_irt", _lib.lib().wgdna_run_irt(ctx.h, _lib.ptr(rad), int(rad_n), int(n_therm),
+                                                         float(E_eV), int(seed), C.byref(r)))
+    return _chem_result(r, rad_n, log)
+
+
+def run_chemistry_device(ctx, n_therm, E_eV, log=None, seed=1):
+    """The same IRT on the rad_buf the last transport left in device memory."""
+    r = _lib.IrtResult()
+    _lib.check("wgdna_irt", _lib.lib().wgdna_irt(ctx.h, int(n_therm), float(E_eV), int(seed), C.byref(r)))
+    return _chem_result(r, r.chem_n, log)
+
+
+runChemistryWorker = run_chemistry_worker
