@@ -167,12 +167,14 @@ def run_native(args, ws, rank, local):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     L = _lib.lib()
-    ctx = wgdna.Context(max_primaries=NP, device=local)
+    NPr = args.np
+    ctx = wgdna.Context(max_primaries=NPr, device=local, max_rad=max(NPr * 1600, 1_000_000),
+                        max_sec=max(NPr * 250, 100_000))
     stream = torch.cuda.Stream(device=dev)
     ctx.set_stream(stream.cuda_stream)
     dna = wgdna.build_dna_target()
-    p = wgdna.transport_params(NP, E_EV, 15000.0, 7.5, dna=dna, seed=args.seed, dna_enable=1)
-    p.pid_base = rank * NP
+    p = wgdna.transport_params(NPr, E_EV, 15000.0, 7.5, dna=dna, seed=args.seed, dna_enable=1)
+    p.pid_base = rank * NPr
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
     st = _lib.TransportStats()
@@ -193,13 +195,13 @@ def run_native(args, ws, rank, local):
                 torch.distributed.all_reduce(summary)
 
     # pinned host buffers for the end-to-end path
-    E_host = torch.full((NP,), E_EV, dtype=torch.float32, pin_memory=True)
-    res_h = torch.empty(NP * 8, dtype=torch.float32, pin_memory=True)
+    E_host = torch.full((NPr,), E_EV, dtype=torch.float32, pin_memory=True)
+    res_h = torch.empty(NPr * 8, dtype=torch.float32, pin_memory=True)
     dose_h = torch.empty(ctx.vc ** 3, dtype=torch.int32, pin_memory=True)
-    rad_cap = 8_000_000
+    rad_cap = ctx.max_rad
     rad_h = torch.empty(rad_cap * 4, dtype=torch.float32, pin_memory=True)
-    p_e2e = wgdna.transport_params(NP, E_EV, 15000.0, 7.5, dna=dna, seed=args.seed, dna_enable=1)
-    p_e2e.pid_base = rank * NP
+    p_e2e = wgdna.transport_params(NPr, E_EV, 15000.0, 7.5, dna=dna, seed=args.seed, dna_enable=1)
+    p_e2e.pid_base = rank * NPr
     p_e2e.E_per_primary = E_host.data_ptr()
     rad_n = C.c_uint64()
     e2e_bytes = {"h2d": 0, "d2h": 0}
@@ -211,8 +213,8 @@ def run_native(args, ws, rank, local):
                                          C.byref(rad_n), C.byref(st)))
         _lib.check("wgdna_irt", L.wgdna_irt(ctx.h, st.n_therm, E_EV, args.seed + 1, C.byref(ir)))
         _lib.check("wgdna_score", L.wgdna_score(ctx.h, 0x12345678, C.byref(ssb), C.byref(dsb)))
-        e2e_bytes["h2d"] = NP * 4 + C.sizeof(p_e2e)
-        e2e_bytes["d2h"] = (NP * 32 + ctx.vc ** 3 * 4 + min(rad_n.value, rad_cap) * 16 + C.sizeof(st) +
+        e2e_bytes["h2d"] = NPr * 4 + C.sizeof(p_e2e)
+        e2e_bytes["d2h"] = (NPr * 32 + ctx.vc ** 3 * 4 + min(rad_n.value, rad_cap) * 16 + C.sizeof(st) +
                             C.sizeof(ir) + C.sizeof(ssb) + C.sizeof(dsb))
 
     for _ in range(args.warmup):
@@ -248,7 +250,7 @@ def run_native(args, ws, rank, local):
         t = torch.tensor([tot_ms], dtype=torch.float64, device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         tot_ms = float(t.item())
-    value = ws * NP * args.steps / (tot_ms / 1000.0)
+    value = ws * NPr * args.steps / (tot_ms / 1000.0)
 
     # end-to-end through the public host API
     for _ in range(2):
@@ -263,7 +265,7 @@ def run_native(args, ws, rank, local):
         t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e_value = ws * NP * args.steps / e2e_s
+    e2e_value = ws * NPr * args.steps / e2e_s
 
     # roofline of the dominant kernel: algorithmic bytes per launch / its mean duration
     pk = peaks()
@@ -272,7 +274,7 @@ def run_native(args, ws, rank, local):
     dom = max(stages, key=stages.get)
     R, S = st.rad_n_stored, st.sec_n
     if dom == "transport":
-        alg = 16 * R + 8 * R + 96 * S + 32 * NP + 4 * st.steps / 50.0
+        alg = 16 * R + 8 * R + 96 * S + 32 * NPr
     elif dom == "irt":
         alg = 16 * R + 34 * R + 16 * ir.n_events
     else:
@@ -291,7 +293,8 @@ def run_native(args, ws, rank, local):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 transport / f64 IRT", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "np_per_gpu": NP, "E_eV": E_EV, "seed": args.seed,
+            "config": {"workload": WORKLOAD if NPr == NP else WORKLOAD.replace("4096", str(NPr)),
+                       "np_per_gpu": NPr, "E_eV": E_EV, "seed": args.seed,
                        "l2": "256 MB write between timed steps (outside the events)",
                        "parallelism": f"primary shards x{ws}"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": e2e_bytes["h2d"],
@@ -324,6 +327,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["native", "reference"], default="native")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--np", type=int, default=NP, help="primaries per GPU per step (4096 = the benchmark)")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     ws, rank, local = dist_init(args)

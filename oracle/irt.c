@@ -387,6 +387,7 @@ static void run_track(const float *rad, const uint64_t *idx, uint32_t n, uint32_
                 if (r2i < 0) continue;
                 double Dj = IRT_D[s2];
                 double dt = ev.t - w->tb[jj];
+                acc->pairs++;
                 double xj = w->px[jj], yj = w->py[jj], zj = w->pz[jj];
                 om_u4 q0 = om_philox(id, jj, pid, 5u, g.k0, g.k1);
                 if (dt > 0) {
@@ -402,7 +403,6 @@ static void run_track(const float *rad, const uint64_t *idx, uint32_t n, uint32_
                 double dx = w->px[id] - xj, dy = w->py[id] - yj, dz = w->pz[id] - zj;
                 double r2 = dx * dx + dy * dy + dz * dz;
                 if (r2 > C.r_cut2) continue;
-                acc->pairs++;
                 double r0 = sqrt(r2);
                 double U = om_u01d32(q0.v[3]);
                 double t = sample_irt(&g, id, jj, r0, r2i, Di + Dj, U);

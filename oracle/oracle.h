@@ -68,7 +68,7 @@ typedef struct {
     double G[7][5];         /* G values per 100 eV of n_therm*E_eV */
     uint64_t rxn_counts[9];
     uint64_t n_reacted;
-    uint64_t n_pairs;       /* reactive pairs inside R_CUT evaluated */
+    uint64_t n_pairs;       /* initial reactive pairs inside R_CUT + (product, partner) reactive pairs */
     uint64_t n_tracks;
     uint64_t n_events;      /* heap pops */
 } orc_irt_out;

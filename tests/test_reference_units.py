@@ -43,7 +43,7 @@ def test_dna_geometry_host_equals_oracle():
 
 
 def decode(w):                                             # rad-buf-encoding.test.ts:20-24
-    i = int(np.floor(w + 0.5))
+    i = int(np.floor(float(w) + 0.5))
     return i // 8, i % 8
 
 

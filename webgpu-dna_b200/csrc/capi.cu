@@ -13,7 +13,7 @@
 #include "transport.cuh"
 
 namespace wg {
-int tables_load(const char* path, Tables* out, float** d_small, float** d_xwc, float** d_xwt);
+int tables_load(const char* path, Tables* out, float** d_small, float2** d_xcw);
 }
 
 using namespace wg;
@@ -33,7 +33,8 @@ struct wgdna_ctx {
     cudaStream_t stream = nullptr, own = nullptr;
     wgdna_cfg cfg{};
     Tables tab{};
-    float *d_small = nullptr, *d_xwc = nullptr, *d_xwt = nullptr;
+    float* d_small = nullptr;
+    float2* d_xcw = nullptr;
     // transport
     float* d_results = nullptr;
     uint32_t* d_dose = nullptr;
@@ -70,7 +71,7 @@ struct wgdna_ctx {
     int8_t* d_sp = nullptr;
     uint8_t* d_alive8 = nullptr;
     double* d_evt = nullptr;
-    int2* d_evab = nullptr;
+    uint32_t* d_evab = nullptr;
     uint32_t* d_track_next = nullptr;
     double* d_acc_tl = nullptr;
     unsigned long long* d_acc = nullptr;
@@ -145,7 +146,7 @@ extern "C" int wgdna_create(const wgdna_cfg* cfg, wgdna_ctx** out) {
     c->cfg = c0;
     std::string tp = c0.tables_path ? std::string(c0.tables_path) : lib_dir() + "/data/cross_sections.bin";
     c->cfg.tables_path = nullptr;
-    int rc = tables_load(tp.c_str(), &c->tab, &c->d_small, &c->d_xwc, &c->d_xwt);
+    int rc = tables_load(tp.c_str(), &c->tab, &c->d_small, &c->d_xcw);
     if (rc != WGDNA_OK) { delete c; return rc; }
     cudaError_t e = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
     if (e != cudaSuccess) { wg_set_error("cudaStreamCreate: %s", cudaGetErrorString(e)); delete c; return WGDNA_ERR_CUDA; }
@@ -177,7 +178,7 @@ extern "C" void wgdna_destroy(wgdna_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    void* ptrs[] = {c->d_small, c->d_xwc, c->d_xwt, c->d_results, c->d_dose, c->d_rad_raw, c->d_key, c->d_rad,
+    void* ptrs[] = {c->d_small, c->d_xcw, c->d_results, c->d_dose, c->d_rad_raw, c->d_key, c->d_rad,
                     c->d_perm, c->d_secq, c->d_st, c->d_Eprim, c->d_pid_cnt, c->d_pid_off, c->d_pid_cur,
                     c->d_red, c->d_err, c->d_fy, c->d_fz, c->d_rbb0, c->d_rbb1, c->d_hits, c->d_alive,
                     c->sc.info, c->sc.last_brk, c->sc.cnt0, c->sc.cnt1, c->sc.cs_in, c->sc.base, c->sc.u64,
@@ -257,7 +258,7 @@ extern "C" int wgdna_transport(wgdna_ctx* c, const wgdna_transport_params* p, wg
     DevState hs;
     WG_CUDA_OK(cudaMemcpyAsync(&hs, c->d_st, sizeof hs, cudaMemcpyDeviceToHost, s));
     WG_CUDA_OK(cudaStreamSynchronize(s));
-    unsigned long long stored = hs.rad_next < c->cfg.max_rad ? hs.rad_next : c->cfg.max_rad;
+    unsigned long long stored = hs.rad_next.v < c->cfg.max_rad ? hs.rad_next.v : c->cfg.max_rad;
     WG_CUDA_OK(cudaEventRecord(c->ev[2], s));
     WG_CUDA_OK(launch_canon(c->d_key, c->d_rad_raw, stored, p->np, c->d_pid_cnt, c->d_pid_off, c->d_pid_cur,
                             c->d_perm, c->d_rad, c->d_err, s));
@@ -273,13 +274,13 @@ extern "C" int wgdna_transport(wgdna_ctx* c, const wgdna_transport_params* p, wg
         memcpy(st->counters, hs.counters, sizeof st->counters);
         memcpy(st->sec_stats, hs.sec_stats, sizeof st->sec_stats);
         memcpy(st->dbg, hs.dbg, sizeof st->dbg);
-        st->counters[6] = hs.sec_tail;
-        st->counters[7] = (uint32_t)hs.rad_next;
-        st->rad_n_raw = hs.rad_next;
+        st->counters[6] = hs.sec_tail.v;
+        st->counters[7] = (uint32_t)hs.rad_next.v;
+        st->rad_n_raw = hs.rad_next.v;
         st->rad_n_stored = stored;
-        st->rad_dropped = hs.rad_next - stored;
-        st->sec_n_raw = hs.sec_tail;
-        st->sec_n = hs.sec_tail < c->cfg.max_sec ? hs.sec_tail : c->cfg.max_sec;
+        st->rad_dropped = hs.rad_next.v - stored;
+        st->sec_n_raw = hs.sec_tail.v;
+        st->sec_n = hs.sec_tail.v - hs.sec_drop;
         st->sec_dropped = hs.sec_drop;
         st->dep_units = red[0];
         st->dep_eV_f64 = hs.dep_f64;
@@ -329,9 +330,9 @@ static void irt_constants(IrtConst* C);
 static int irt_ensure(wgdna_ctx* c, uint32_t cap) {
     int blocks = irt_blocks(c->device);
     uint32_t warps = (uint32_t)blocks * 4u;
-    uint32_t ecap = cap * 16u;
+    uint32_t ecap = cap * 4u + 4096u;     // events per track: ~1.3 per particle at 10 keV
     if (cap <= c->irt_cap && warps <= c->irt_warps && ecap <= c->irt_ecap) return WGDNA_OK;
-    size_t nn = (size_t)warps * cap, ne = (size_t)warps * ecap;
+    size_t nn = (size_t)warps * cap, ne = (size_t)warps * 2 * ecap;
     TRY(dalloc(&c->d_px, nn)); TRY(dalloc(&c->d_py, nn)); TRY(dalloc(&c->d_pz, nn)); TRY(dalloc(&c->d_tb, nn));
     TRY(dalloc(&c->d_sp, nn)); TRY(dalloc(&c->d_alive8, nn));
     TRY(dalloc(&c->d_evt, ne)); TRY(dalloc(&c->d_evab, ne));
@@ -359,6 +360,10 @@ static int irt_run(wgdna_ctx* c, uint32_t nseg, uint32_t n_therm, double E_eV, u
     WG_CUDA_OK(cudaStreamSynchronize(s));
     if (maxseg > (1ull << 24)) { wg_set_error("wgdna_irt: track of %llu entries is too large", maxseg); return WGDNA_ERR_CAPACITY; }
     uint32_t cap = (uint32_t)(2 * maxseg + 512);
+    if (cap > 65535u) {
+        wg_set_error("wgdna_irt: a track of %llu entries exceeds the 32,511-entry limit of the event encoding", maxseg);
+        return WGDNA_ERR_CAPACITY;
+    }
     TRY(irt_ensure(c, cap));
     WG_CUDA_OK(cudaMemsetAsync(c->d_track_next, 0, 4, s));
     WG_CUDA_OK(cudaMemsetAsync(c->d_acc_tl, 0, 35 * 8, s));
@@ -456,6 +461,7 @@ static void irt_constants(IrtConst* C) {
             double sig = k / (4 * M_PI * Ds);
             if (self) sig *= 2;
             C->sigma[r] = sig; C->sigma_eff[r] = sig; C->kdif[r] = 0; C->prob[r] = 1;
+            C->acc_s[r] = sig; C->acc_c[r] = 1.0; C->acc_add[r] = 0.5 * fabs(rc);
         } else {
             double sc = VDW[a] + VDW[b];
             C->sigma[r] = sc;
@@ -465,6 +471,9 @@ static void irt_constants(IrtConst* C) {
             C->sigma_eff[r] = se; C->kdif[r] = kd;
             double ka = kd * k / (kd - k);
             C->prob[r] = Rs / (Rs + (kd / ka) * (se + Rs));
+            C->acc_s[r] = rc == 0 ? sc : se;
+            C->acc_c[r] = k / kd;
+            C->acc_add[r] = 0.5 * fabs(rc);
             if (rc == 0) {
                 C->a_pdc[r] = (1.0 / sc) * ka / k;
             } else {

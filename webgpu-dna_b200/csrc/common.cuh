@@ -21,9 +21,8 @@ enum : uint32_t {
 // Cross-section tables (public/cross_sections.wgsl:9-72) in device memory.
 struct Tables {
     // small tables, copied to shared memory by the transport kernel, in this order
-    const float* small;            // see SMALL_* offsets
-    const float* xwc;              // 5 x (N_WE*N_WR) Born CDF
-    const float* xwt;              // 5 x (N_WE*N_WR) Born energy transfer
+    const float* small;            // see the S_* offsets
+    const float2* xcw;             // 5 x (N_WE*N_WR) (Born CDF, energy transfer) pairs
     float log_xe0, inv_log_xe_step, log_xae0, inv_log_xae_step;
     uint32_t xn, n_ae, n_ac, n_we, n_wr, n_vib;
 };
@@ -43,25 +42,31 @@ constexpr int S_XVE = S_XWE + NWE_;
 constexpr int S_XVS = S_XVE + NVIB_;
 constexpr int S_XVMF = S_XVS + NVIB_;      // 38 x 9
 constexpr int S_VIB = S_XVMF + NVIB_ * 9;  // 9
-constexpr int S_TOTAL = S_VIB + 9;
+constexpr int S_GUIDE = S_VIB + 9;         // 5 x 58 x 16: Born CDF at breakpoints 0, 16, ..., 240
+constexpr int GUIDES = 16;
+constexpr int S_TOTAL = S_GUIDE + 5 * NWE_ * GUIDES;
 constexpr int S_TOTAL_PAD = (S_TOTAL + 3) & ~3;
 
 // Global state of one transport run (device memory, zeroed before the run).
+// The counters that many warps update or poll each sit on their own 128-byte
+// line so that polling one does not stall atomics on another.
+struct __align__(128) Line32 { uint32_t v; uint32_t pad[31]; };
+struct __align__(128) Line64 { unsigned long long v; unsigned long long pad[15]; };
 struct DevState {
     uint32_t counters[8];      // primary.wgsl:24-35 semantics
     uint32_t sec_stats[8];     // secondary.wgsl sec_stats
     uint32_t dbg[8];           // primary.wgsl dbg (dbg[2] = escaped count)
-    unsigned long long rad_next;   // rad_buf slots reserved (may exceed capacity)
     unsigned long long rad_drop;   // rad_buf entries dropped at capacity
     unsigned long long steps;      // electron steps taken
     double dep_f64;                // every deposit, f64
-    uint32_t sec_tail;             // secondaries reserved
-    uint32_t sec_head;             // secondaries taken
     uint32_t sec_drop;             // secondaries dropped at capacity
-    uint32_t prim_next;            // primaries taken
-    int live;                      // particles started and not finished
     uint32_t err;
-    uint32_t pad[2];
+    Line64 rad_next;               // rad_buf slots reserved (may exceed capacity)
+    Line32 sec_tail;               // secondaries emitted (counters[6])
+    Line32 sec_qtail;              // secondaries placed in the global queue
+    Line32 sec_head;               // queued secondaries taken
+    Line32 prim_next;              // primaries taken
+    Line32 busy;                   // warps holding work
 };
 
 // One queued secondary (the Particle struct of primary.wgsl:14, with the
@@ -71,6 +76,9 @@ struct __align__(16) SecRec {
     float4 dir;       // dx, dy, dz, (unused)
     uint4 meta;       // pid, sub, epoch (ready flag), 0
 };
+
+// A secondary waiting in a warp's shared-memory stash.
+struct StashRec { float x, y, z, E, dx, dy, dz; uint32_t pid, sub; };
 
 }  // namespace wg
 

@@ -70,28 +70,39 @@ __device__ __forceinline__ double erfcx_(double x) {
     return erfcx_pos(x);
 }
 
-__device__ __noinline__ double sample_pdc(uint32_t i, uint32_t j, uint32_t pid, uint32_t k0, uint32_t k1,
-                                          double a, double b) {                // :91-113
+// SamplePDC (:91-113) for one pair, 32 trials at a time across the warp; the
+// first accepted trial in trial order wins, as in the sequential loop.  Must
+// be called by all 32 lanes with the same arguments.
+__device__ double pdc_warp(uint32_t i, uint32_t j, uint32_t pid, uint32_t k0, uint32_t k1, double a, double b,
+                           int lane) {
     double p = 2.0 * sqrt(2.0 * b / a);
     double q = 2.0 / sqrt(2.0 * b / a);
     double M = fmax(1.0 / (a * a), 3.0 * b / a);
-    for (uint32_t trial = 0; trial < 10000; ++trial) {
-        u4 w = philox(i, j, pid, 4u | (trial << 4), k0, k1);
-        double U = u01d(w.x, w.y);
-        double X;
-        if (U < p / (p + q * M)) { double h = U * (p + q * M) / 2; X = h * h; }
-        else { double h = 2 / ((1 - U) * (p + q * M) / M); X = h * h; }
-        U = u01d(w.z, w.w);
-        double sqX = sqrt(X);
-        double lambdax = exp_(-b * b / X) * (1.0 - a * sqrt(3.141592653589793 * X) * erfcx_(b / sqX + a * sqX));
-        if ((X <= 2.0 * b / a && U <= lambdax) || (X >= 2.0 * b / a && U * M / X <= lambdax)) return X;
+    for (uint32_t t0 = 0; t0 < 10000; t0 += 32) {
+        uint32_t trial = t0 + lane;
+        bool ok = false;
+        double X = 0;
+        if (trial < 10000) {
+            u4 w = philox(i, j, pid, 4u | (trial << 4), k0, k1);
+            double U = u01d(w.x, w.y);
+            if (U < p / (p + q * M)) { double h = U * (p + q * M) / 2; X = h * h; }
+            else { double h = 2 / ((1 - U) * (p + q * M) / M); X = h * h; }
+            U = u01d(w.z, w.w);
+            double sqX = sqrt(X);
+            double lambdax = exp_(-b * b / X) * (1.0 - a * sqrt(3.141592653589793 * X) * erfcx_(b / sqX + a * sqX));
+            ok = (X <= 2.0 * b / a && U <= lambdax) || (X >= 2.0 * b / a && U * M / X <= lambdax);
+        }
+        unsigned m = __ballot_sync(0xffffffffu, ok);
+        if (m) return __shfl_sync(0xffffffffu, X, __ffs(m) - 1);
     }
     return -1.0;
 }
 
-// sampleIRT (:116-184) with the acceptance draw U supplied
-__device__ __forceinline__ double sample_irt(const IrtConst& C, uint32_t i, uint32_t j, uint32_t pid,
-                                             uint32_t k0, uint32_t k1, double r0, int ri, double D, double U) {
+// sampleIRT (:116-184) with the acceptance draw U supplied.  Returns the
+// reaction time t >= 0, -1 for no reaction, or -2 when SamplePDC must be run
+// with (*pa, *pb); the caller then uses X / D for X > 0.
+__device__ __forceinline__ double sample_pre(const IrtConst& C, double r0, int ri, double D, double U,
+                                             double* pa, double* pb) {
     if (C.type[ri] == 0) {
         double sigma = C.sigma[ri], rc = C.rc[ri];
         if (sigma <= 0 || D <= 0) return -1;
@@ -107,7 +118,7 @@ __device__ __forceinline__ double sample_irt(const IrtConst& C, uint32_t i, uint
         return 0.25 * dr * dr / (D * ei * ei);
     }
     double sigma_c = C.sigma[ri], rc = C.rc[ri];
-    double a = C.a_pdc[ri], b, sc_chk = sigma_c, r0_chk = r0;
+    double b, sc_chk = sigma_c, r0_chk = r0;
     if (rc == 0) {
         b = (r0 - sigma_c) / 2;
     } else {
@@ -118,77 +129,131 @@ __device__ __forceinline__ double sample_irt(const IrtConst& C, uint32_t i, uint
     }
     if (sc_chk > r0_chk) return (C.prob[ri] > U) ? 0 : -1;
     double Winf = sc_chk / r0_chk * C.kobs[ri] / C.kdif[ri];
-    if (Winf > U) {
-        double X = sample_pdc(i, j, pid, k0, k1, a, b);
-        if (X > 0) return X / D;
-    }
+    if (Winf > U) { *pa = C.a_pdc[ri]; *pb = b; return -2; }
     return -1;
 }
 
-// lane-0 binary heap on (t, a, b)
-__device__ __forceinline__ bool ev_less(double t1, int2 x, double t2, int2 y) {
-    if (t1 != t2) return t1 < t2;
-    if (x.x != y.x) return x.x < y.x;
-    return x.y < y.y;
+// Distance beyond which sample_pre certainly returns -1 for acceptance draw U:
+//   TDC:  Winf = sigma / r0e and r0e >= r0 - max(rc,0)/2      -> r0 < sigma/U + rc/2
+//   PDC:  contact needs r0 < sigma_x, Winf = sigma_x c / r0_chk with r0_chk >= r0
+//         (c = kobs/kdif)                                     -> r0 < max(sigma_x, sigma_x c / U)
+// with a relative and absolute safety margin for rounding.
+__device__ __forceinline__ double r_acc(const IrtConst& C, int ri, double U) {
+    double s = C.acc_s[ri];
+    double R = fmax(s, s * C.acc_c[ri] / U) + C.acc_add[ri];
+    return R * (1.0 + 1e-6) + 1e-6;
 }
-__device__ void heap_sift_down(double* T, int2* AB, uint32_t n, uint32_t p) {
-    double tp = T[p];
-    int2 ap = AB[p];
+
+// event heap on (t, packed a<<16|b); nodes [0, HS) in shared memory, the rest in global memory
+constexpr uint32_t HS = 512;
+struct Heap {
+    double* st; uint32_t* sab; double* gt; uint32_t* gab;
+    __device__ __forceinline__ double t(uint32_t k) const { return k < HS ? st[k] : gt[k - HS]; }
+    __device__ __forceinline__ uint32_t ab(uint32_t k) const { return k < HS ? sab[k] : gab[k - HS]; }
+    __device__ __forceinline__ void set(uint32_t k, double tv, uint32_t abv) const {
+        if (k < HS) { st[k] = tv; sab[k] = abv; } else { gt[k - HS] = tv; gab[k - HS] = abv; }
+    }
+};
+__device__ __forceinline__ bool ev_less(double t1, uint32_t x, double t2, uint32_t y) {
+    return t1 != t2 ? t1 < t2 : x < y;
+}
+__device__ void heap_push(const Heap& H, uint32_t& n, double t, uint32_t ab) {
+    uint32_t c = n++;
+    while (c > 0) {
+        uint32_t p = (c - 1) >> 1;
+        double tp = H.t(p);
+        uint32_t ap = H.ab(p);
+        if (!ev_less(t, ab, tp, ap)) break;
+        H.set(c, tp, ap);
+        c = p;
+    }
+    H.set(c, t, ab);
+}
+__device__ void heap_pop(const Heap& H, uint32_t& n) {
+    n--;
+    if (n == 0) return;
+    double tp = H.t(n);
+    uint32_t ap = H.ab(n);
+    uint32_t p = 0;
     for (;;) {
         uint32_t l = 2 * p + 1;
         if (l >= n) break;
         uint32_t s = l;
-        double ts = T[l];
-        int2 as = AB[l];
+        double ts = H.t(l);
+        uint32_t as = H.ab(l);
         if (l + 1 < n) {
-            double tr = T[l + 1];
-            int2 ar = AB[l + 1];
+            double tr = H.t(l + 1);
+            uint32_t ar = H.ab(l + 1);
             if (ev_less(tr, ar, ts, as)) { s = l + 1; ts = tr; as = ar; }
         }
         if (!ev_less(ts, as, tp, ap)) break;
-        T[p] = ts; AB[p] = as;
+        H.set(p, ts, as);
         p = s;
     }
-    T[p] = tp; AB[p] = ap;
+    H.set(p, tp, ap);
 }
-__device__ void heap_push(double* T, int2* AB, uint32_t& n, double t, int2 ab) {
-    uint32_t c = n++;
-    while (c > 0) {
-        uint32_t p = (c - 1) >> 1;
-        if (!ev_less(t, ab, T[p], AB[p])) break;
-        T[c] = T[p]; AB[c] = AB[p];
-        c = p;
+
+// warp bitonic sort of n events (t, ab) in global memory, ascending
+__device__ void warp_sort(double* T, uint32_t* AB, uint32_t n, int lane) {
+    uint32_t n2 = 1;
+    while (n2 < n) n2 <<= 1;
+    for (uint32_t k = n + lane; k < n2; k += 32) { T[k] = 1e300; AB[k] = 0xffffffffu; }
+    __syncwarp();
+    for (uint32_t k = 2; k <= n2; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = lane; i < n2; i += 32) {
+                uint32_t l = i ^ j;
+                if (l > i) {
+                    double ti = T[i], tl = T[l];
+                    uint32_t ai = AB[i], al = AB[l];
+                    bool up = (i & k) == 0;
+                    if (ev_less(tl, al, ti, ai) == up) { T[i] = tl; T[l] = ti; AB[i] = al; AB[l] = ai; }
+                }
+            }
+            __syncwarp();
+            __threadfence_block();
+        }
     }
-    T[c] = t; AB[c] = ab;
 }
+
+constexpr uint32_t FULL = 0xffffffffu;
 
 __global__ void __launch_bounds__(IB) k_irt(IArgs A) {
     __shared__ double s_tl[IB / 32][35];
+    __shared__ double s_ht[IB / 32][HS];
+    __shared__ uint32_t s_hab[IB / 32][HS];
     __shared__ IrtConst s_c;
+    __shared__ uint32_t s_row[6];
     for (int k = threadIdx.x; k < (int)(sizeof(IrtConst) / 4); k += IB)
         reinterpret_cast<uint32_t*>(&s_c)[k] = reinterpret_cast<const uint32_t*>(&c_irt)[k];
     __syncthreads();
+    if (threadIdx.x < 6) {
+        uint32_t row = 0;           // reaction index of (s, q) in 4-bit fields, 15 = none
+        for (int q = 5; q >= 0; --q) row = (row << 4) | (uint32_t)(s_c.map[threadIdx.x * 6 + q] & 15);
+        s_row[threadIdx.x] = row;
+    }
     const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     const uint32_t gw = blockIdx.x * (IB / 32) + wl;
     const IrtConst& C = s_c;
     for (int k = lane; k < 35; k += 32) s_tl[wl][k] = 0.0;
+    __syncthreads();
     double* px = A.px + (size_t)gw * A.cap;
     double* py = A.py + (size_t)gw * A.cap;
     double* pz = A.pz + (size_t)gw * A.cap;
     double* tb = A.tb + (size_t)gw * A.cap;
     int8_t* sp = A.sp + (size_t)gw * A.cap;
     uint8_t* alive = A.alive + (size_t)gw * A.cap;
-    double* HT = A.ev_t + (size_t)gw * A.ecap;
-    int2* HAB = A.ev_ab + (size_t)gw * A.ecap;
+    double* ET = A.ev_t + (size_t)gw * 2 * A.ecap;          // [0, ecap): initial events
+    uint32_t* EAB = A.ev_ab + (size_t)gw * 2 * A.ecap;
+    Heap H{s_ht[wl], s_hab[wl], ET + A.ecap, EAB + A.ecap};  // product events
     unsigned long long rxn[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     unsigned long long n_reacted = 0, n_pairs = 0, n_events = 0, n_tracks = 0;
-    const double CP[7] = {0.001, 0.01, 0.1, 1, 10, 100, 1000};
 
     for (;;) {
         uint32_t p = 0;
         if (lane == 0) p = atomicAdd(A.track_next, 1u);
-        p = __shfl_sync(0xffffffffu, p, 0);
+        p = __shfl_sync(FULL, p, 0);
         if (p >= A.nseg) break;
         unsigned long long s = A.seg_off[p], e = A.seg_off[p + 1];
         if (s == e) continue;
@@ -203,8 +268,8 @@ __global__ void __launch_bounds__(IB) k_irt(IArgs A) {
             float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
             if (valid) { r = A.rad[idx]; code = (int)rintf(r.w) % 8; }
             bool keep = valid && code >= 0 && code != 4 && code != 7;
-            h2 += __popc(__ballot_sync(0xffffffffu, valid && code == 7));
-            unsigned m = __ballot_sync(0xffffffffu, keep);
+            h2 += __popc(__ballot_sync(FULL, valid && code == 7));
+            unsigned m = __ballot_sync(FULL, keep);
             uint32_t k = n + __popc(m & lt);
             if (keep && k < A.cap) {
                 double x = r.x, y = r.y, z = r.z;
@@ -239,17 +304,16 @@ __global__ void __launch_bounds__(IB) k_irt(IArgs A) {
             if (keep && k >= A.cap) overflow = true;
             n += __popc(m);
         }
-        if (__any_sync(0xffffffffu, overflow)) { if (lane == 0) atomicOr(A.err, DERR_TRACK_SIZE); continue; }
+        if (__any_sync(FULL, overflow)) { if (lane == 0) atomicOr(A.err, DERR_TRACK_SIZE); continue; }
         if (n == 0) continue;
         n_tracks++;
         __syncwarp();
         __threadfence_block();
-        // alive counts per species (lane 0 keeps them)
         uint32_t cnt[6] = {0, 0, 0, 0, 0, 0};
         for (uint32_t c = 0; c < n; c += 32) {
             uint32_t k = c + lane;
             int spc = k < n ? sp[k] : -1;
-            for (int q = 0; q < 6; ++q) cnt[q] += __popc(__ballot_sync(0xffffffffu, spc == q));
+            for (int q = 0; q < 6; ++q) cnt[q] += __popc(__ballot_sync(FULL, spc == q));
         }
         // -------------------------------------------------- initial pairing (:539-558)
         uint32_t nev = 0;
@@ -260,72 +324,98 @@ __global__ void __launch_bounds__(IB) k_irt(IArgs A) {
             double xi = 0, yi = 0, zi = 0, Di = 0;
             int si = 0;
             if (hi) { xi = px[i]; yi = py[i]; zi = pz[i]; si = sp[i]; Di = C.D[si]; }
-            uint32_t row = 0;                      // reaction index of (si, s) in 4-bit fields, 15 = none
-            for (int q = 5; q >= 0; --q) row = (row << 4) | (uint32_t)(C.map[si * 6 + q] & 15);
+            uint32_t row = s_row[si];
             uint32_t cblk = 0xffffffffu;
             u4 cw = {0, 0, 0, 0};
-            for (uint32_t j = i0 + 1; j < n; ++j) {
-                bool acc = false;
-                double t = 0;
-                if (hi && j > i) {
-                    int sj = sp[j];
-                    int ri = (int)((row >> (4 * sj)) & 15u);
-                    if (ri != 15) {
-                        double dx = xi - px[j], dy = yi - py[j], dz = zi - pz[j];
-                        double r2 = dx * dx + dy * dy + dz * dz;
-                        if (r2 <= C.r_cut2) {
-                            n_pairs++;
-                            double r0 = sqrt(r2);
-                            if ((j >> 2) != cblk) { cblk = j >> 2; cw = philox(cblk, i, pid, 3u, A.k0, A.k1); }
-                            uint32_t wd = (j & 3) == 0 ? cw.x : (j & 3) == 1 ? cw.y : (j & 3) == 2 ? cw.z : cw.w;
-                            double U = u01d32(wd);
-                            t = sample_irt(C, i, j, pid, A.k0, A.k1, r0, ri, Di + C.D[sj], U);
-                            acc = (t >= 0 && t < 1000);
+            for (uint32_t j0 = i0; j0 < n; j0 += 32) {
+                uint32_t jl = j0 + lane;
+                double cx = 0, cy = 0, cz = 0;
+                int cs = 0;
+                if (jl < n) { cx = px[jl]; cy = py[jl]; cz = pz[jl]; cs = sp[jl]; }
+                uint32_t kmax = min(32u, n - j0);
+                for (uint32_t kk = 0; kk < kmax; ++kk) {
+                    uint32_t j = j0 + kk;
+                    double xj = __shfl_sync(FULL, cx, kk), yj = __shfl_sync(FULL, cy, kk), zj = __shfl_sync(FULL, cz, kk);
+                    int sj = __shfl_sync(FULL, cs, kk);
+                    bool acc = false, pdcq = false;
+                    double t = 0, pa = 0, pb = 0, pD = 0;
+                    if (hi && j > i) {
+                        int ri = (int)((row >> (4 * sj)) & 15u);
+                        if (ri != 15) {
+                            double dx = xi - xj, dy = yi - yj, dz = zi - zj;
+                            double r2 = dx * dx + dy * dy + dz * dz;
+                            if (r2 <= C.r_cut2) {
+                                n_pairs++;
+                                if ((j >> 2) != cblk) { cblk = j >> 2; cw = philox(cblk, i, pid, 3u, A.k0, A.k1); }
+                                uint32_t wd = (j & 3) == 0 ? cw.x : (j & 3) == 1 ? cw.y : (j & 3) == 2 ? cw.z : cw.w;
+                                double U = u01d32(wd);
+                                double R = r_acc(C, ri, U);
+                                if (r2 <= R * R) {
+                                    double D = Di + C.D[sj];
+                                    t = sample_pre(C, sqrt(r2), ri, D, U, &pa, &pb);
+                                    if (t == -2.0) { pdcq = true; pD = D; }
+                                    else acc = (t >= 0 && t < 1000);
+                                }
+                            }
                         }
                     }
-                }
-                unsigned m = __ballot_sync(0xffffffffu, acc);
-                if (m) {
-                    uint32_t slot = nev + __popc(m & lt);
-                    if (acc) {
-                        if (slot < A.ecap) { HT[slot] = t; HAB[slot] = make_int2((int)i, (int)j); }
-                        else ev_over = true;
+                    unsigned pm = __ballot_sync(FULL, pdcq);
+                    while (pm) {
+                        int src = __ffs(pm) - 1;
+                        pm &= pm - 1;
+                        uint32_t qi = __shfl_sync(FULL, i, src);
+                        double qa = __shfl_sync(FULL, pa, src), qb = __shfl_sync(FULL, pb, src);
+                        double X = pdc_warp(qi, j, pid, A.k0, A.k1, qa, qb, lane);
+                        if (lane == src && X > 0) { t = X / pD; acc = t < 1000; }
                     }
-                    nev += __popc(m);
+                    unsigned m = __ballot_sync(FULL, acc);
+                    if (m) {
+                        uint32_t slot = nev + __popc(m & lt);
+                        if (acc) {
+                            if (slot < A.ecap) { ET[slot] = t; EAB[slot] = (i << 16) | j; }
+                            else ev_over = true;
+                        }
+                        nev += __popc(m);
+                    }
                 }
             }
         }
-        if (__any_sync(0xffffffffu, ev_over)) { if (lane == 0) atomicOr(A.err, DERR_HEAP); continue; }
+        if (__any_sync(FULL, ev_over)) { if (lane == 0) atomicOr(A.err, DERR_HEAP); continue; }
         __syncwarp();
         __threadfence_block();
+        warp_sort(ET, EAB, nev, lane);
         // ------------------------------------------------------- event loop (:566-660)
-        uint32_t hn = nev;
-        if (lane == 0) for (int k = (int)hn / 2 - 1; k >= 0; --k) heap_sift_down(HT, HAB, hn, (uint32_t)k);
+        uint32_t ip = 0, hn = 0;
         uint32_t ntot = n;
         double h2c = (double)h2;
         int cp = 0;
         bool heap_over = false;
+        const double CP[7] = {0.001, 0.01, 0.1, 1, 10, 100, 1000};
         for (;;) {
-            hn = __shfl_sync(0xffffffffu, hn, 0);
-            if (hn == 0) break;
             double et = 0;
-            int ei = 0, ej = 0;
+            uint32_t eab = 0;
+            int have = 0;
             if (lane == 0) {
-                et = HT[0]; int2 ab = HAB[0];
-                ei = ab.x; ej = ab.y;
-                hn--;
-                if (hn > 0) { HT[0] = HT[hn]; HAB[0] = HAB[hn]; heap_sift_down(HT, HAB, hn, 0); }
-                n_events++;
-                while (cp < 7 && et >= CP[cp]) {
-                    s_tl[wl][cp * 5 + 0] += cnt[0]; s_tl[wl][cp * 5 + 1] += cnt[1];
-                    s_tl[wl][cp * 5 + 2] += cnt[2]; s_tl[wl][cp * 5 + 3] += cnt[4];
-                    s_tl[wl][cp * 5 + 4] += h2c;
-                    cp++;
+                bool hi_ = ip < nev, hh = hn > 0;
+                if (hi_ || hh) {
+                    have = 1;
+                    double ti = hi_ ? ET[ip] : 0.0, th = hh ? H.t(0) : 0.0;
+                    uint32_t ai = hi_ ? EAB[ip] : 0u, ah = hh ? H.ab(0) : 0u;
+                    if (hi_ && (!hh || ev_less(ti, ai, th, ah))) { et = ti; eab = ai; ip++; }
+                    else { et = th; eab = ah; heap_pop(H, hn); }
+                    n_events++;
+                    while (cp < 7 && et >= CP[cp]) {
+                        s_tl[wl][cp * 5 + 0] += cnt[0]; s_tl[wl][cp * 5 + 1] += cnt[1];
+                        s_tl[wl][cp * 5 + 2] += cnt[2]; s_tl[wl][cp * 5 + 3] += cnt[4];
+                        s_tl[wl][cp * 5 + 4] += h2c;
+                        cp++;
+                    }
                 }
             }
-            et = __shfl_sync(0xffffffffu, et, 0);
-            ei = __shfl_sync(0xffffffffu, ei, 0);
-            ej = __shfl_sync(0xffffffffu, ej, 0);
+            if (!__shfl_sync(FULL, have, 0)) break;
+            et = __shfl_sync(FULL, et, 0);
+            eab = __shfl_sync(FULL, eab, 0);
+            int ei = (int)(eab >> 16), ej = (int)(eab & 0xffffu);
             int valid = 0, si = 0, sj = 0, ri = -1;
             if (lane == 0) {
                 if (alive[ei] && alive[ej]) {
@@ -341,11 +431,11 @@ __global__ void __launch_bounds__(IB) k_irt(IArgs A) {
                     }
                 }
             }
-            valid = __shfl_sync(0xffffffffu, valid, 0);
+            valid = __shfl_sync(FULL, valid, 0);
             if (!valid) continue;
-            si = __shfl_sync(0xffffffffu, si, 0);
-            sj = __shfl_sync(0xffffffffu, sj, 0);
-            ri = __shfl_sync(0xffffffffu, ri, 0);
+            si = __shfl_sync(FULL, si, 0);
+            sj = __shfl_sync(FULL, sj, 0);
+            ri = __shfl_sync(FULL, ri, 0);
             int np_ = C.nprod[ri];
             if (np_ == 0) continue;
             double sqDi = sqrt(C.D[si]), sqDj = sqrt(C.D[sj]);
@@ -373,47 +463,72 @@ __global__ void __launch_bounds__(IB) k_irt(IArgs A) {
                 __threadfence_block();
                 // pairWithAlive (:430-465)
                 double Di = C.D[nsp];
+                uint32_t rowp = s_row[nsp];
                 for (uint32_t c0 = 0; c0 < ntot; c0 += 32) {
                     uint32_t jj = c0 + lane;
-                    bool acc = false;
-                    double ta = 0;
-                    if (jj < ntot && jj != id && alive[jj]) {
-                        int s2 = sp[jj];
-                        int r2i = C.map[nsp * 6 + s2];
-                        if (r2i >= 0) {
-                            double Dj = C.D[s2];
-                            double dt = et - tb[jj];
-                            double xj = px[jj], yj = py[jj], zj = pz[jj];
-                            u4 q0 = philox(id, jj, pid, 5u, A.k0, A.k1);
-                            if (dt > 0) {
-                                double sig = sqrt(2.0 * Dj * dt);
+                    bool cand = jj < ntot && jj != id && alive[jj];
+                    int s2 = cand ? sp[jj] : 0;
+                    int r2i = (int)((rowp >> (4 * s2)) & 15u);
+                    cand = cand && r2i != 15;
+                    bool acc = false, pdcq = false;
+                    double ta = 0, pa = 0, pb = 0, pD = 0;
+                    if (cand) {
+                        n_pairs++;
+                        double Dj = C.D[s2];
+                        double dt = et - tb[jj];
+                        double xj = px[jj], yj = py[jj], zj = pz[jj];
+                        u4 q0 = philox(id, jj, pid, 5u, A.k0, A.k1);
+                        double U = u01d32(q0.w);
+                        double R = r_acc(C, r2i, U);
+                        bool need = true;
+                        if (dt > 0) {
+                            double sig = sqrt(2.0 * Dj * dt);
+                            // |gaussian 3-vector| <= sqrt(sum -2 ln u1_k) (Box-Muller radius), with margin
+                            float l0 = -2.0f * __logf((float)u01d32(q0.x));
+                            float l1 = -2.0f * __logf((float)u01d32(q0.y));
+                            float l2 = -2.0f * __logf((float)u01d32(q0.z));
+                            double B = (double)sqrtf((l0 + l1 + l2) * 1.0001f) + 1e-4;
+                            double ex = nx - xj, ey = ny - yj, ez = nz - zj;
+                            double dist = sqrt(ex * ex + ey * ey + ez * ez);
+                            if (dist - sig * B > R) need = false;
+                            if (need) {
                                 u4 q1 = philox(id, jj, pid, 5u | (1u << 4), A.k0, A.k1);
                                 double g0 = sqrt(-2 * log_(u01d32(q0.x) + 1e-30)) * cos_(6.2831853 * u01d32(q1.x));
                                 double g1 = sqrt(-2 * log_(u01d32(q0.y) + 1e-30)) * cos_(6.2831853 * u01d32(q1.y));
                                 double g2 = sqrt(-2 * log_(u01d32(q0.z) + 1e-30)) * cos_(6.2831853 * u01d32(q1.z));
                                 xj += g0 * sig; yj += g1 * sig; zj += g2 * sig;
                             }
+                        }
+                        if (need) {
                             double dx = nx - xj, dy = ny - yj, dz = nz - zj;
                             double r2 = dx * dx + dy * dy + dz * dz;
                             if (r2 <= C.r_cut2) {
-                                n_pairs++;
-                                double r0 = sqrt(r2);
-                                double U = u01d32(q0.w);
-                                double t = sample_irt(C, id, jj, pid, A.k0, A.k1, r0, r2i, Di + Dj, U);
-                                if (t >= 0) { ta = et + t; acc = ta < 1000; }
+                                double D = Di + Dj;
+                                double t = sample_pre(C, sqrt(r2), r2i, D, U, &pa, &pb);
+                                if (t == -2.0) { pdcq = true; pD = D; }
+                                else if (t >= 0) { ta = et + t; acc = ta < 1000; }
                             }
                         }
                     }
-                    unsigned m = __ballot_sync(0xffffffffu, acc);
+                    unsigned pm = __ballot_sync(FULL, pdcq);
+                    while (pm) {
+                        int src = __ffs(pm) - 1;
+                        pm &= pm - 1;
+                        uint32_t qj = __shfl_sync(FULL, jj, src);
+                        double qa = __shfl_sync(FULL, pa, src), qb = __shfl_sync(FULL, pb, src);
+                        double X = pdc_warp(id, qj, pid, A.k0, A.k1, qa, qb, lane);
+                        if (lane == src && X > 0) { ta = et + X / pD; acc = ta < 1000; }
+                    }
+                    unsigned m = __ballot_sync(FULL, acc);
                     while (m) {
                         int src = __ffs(m) - 1;
                         m &= m - 1;
-                        double tt = __shfl_sync(0xffffffffu, ta, src);
-                        uint32_t pj = __shfl_sync(0xffffffffu, jj, src);
+                        double tt = __shfl_sync(FULL, ta, src);
+                        uint32_t pj = __shfl_sync(FULL, jj, src);
                         if (lane == 0) {
-                            if (hn < A.ecap) {
-                                int a = (int)(pj < id ? pj : id), bq = (int)(pj < id ? id : pj);
-                                heap_push(HT, HAB, hn, tt, make_int2(a, bq));
+                            if (hn < HS + A.ecap) {
+                                uint32_t a = pj < id ? pj : id, bq = pj < id ? id : pj;
+                                heap_push(H, hn, tt, (a << 16) | bq);
                             } else heap_over = true;
                         }
                     }
@@ -433,16 +548,15 @@ __global__ void __launch_bounds__(IB) k_irt(IArgs A) {
         }
         __syncwarp();
     }
-    // per-warp totals -> global
     for (int k = 0; k < 9; ++k) {
         unsigned long long v = rxn[k];
-        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
         if (lane == 0 && v) atomicAdd(&A.acc[k], v);
     }
     unsigned long long vals[4] = {n_reacted, n_pairs, n_events, n_tracks};
     for (int k = 0; k < 4; ++k) {
         unsigned long long v = vals[k];
-        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
         if (lane == 0 && v) atomicAdd(&A.acc[9 + k], v);
     }
     __syncwarp();

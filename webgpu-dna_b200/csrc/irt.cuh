@@ -6,6 +6,7 @@ namespace wg {
 
 struct IrtConst {
     double sigma[9], sigma_eff[9], rc[9], kdif[9], kobs[9], prob[9], a_pdc[9], coth_sig[9];
+    double acc_s[9], acc_c[9], acc_add[9];   // acceptance-radius bound (irt.cu r_acc)
     int type[9], nprod[9], prod0[9], prod1[9];
     int map[36];
     double D[6];
@@ -20,8 +21,8 @@ struct IArgs {
     double *px, *py, *pz, *tb;           // [warp][cap]
     int8_t* sp;
     uint8_t* alive;
-    double* ev_t;                        // [warp][ecap]
-    int2* ev_ab;
+    double* ev_t;                        // [warp][2*ecap]: initial events, then heap overflow
+    uint32_t* ev_ab;                     // packed (a << 16) | b
     uint32_t* track_next;
     double* acc_tl;                      // 35
     unsigned long long* acc;             // [0..8] rxn, 9 reacted, 10 pairs, 11 events, 12 tracks

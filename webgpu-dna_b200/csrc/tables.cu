@@ -25,7 +25,7 @@ static bool find(const std::vector<Entry>& es, const char* name, uint32_t count,
     return false;
 }
 
-int tables_load(const char* path, Tables* out, float** d_small, float** d_xwc, float** d_xwt) {
+int tables_load(const char* path, Tables* out, float** d_small, float2** d_xcw) {
     FILE* f = fopen(path, "rb");
     if (!f) { wg_set_error("cannot open cross-section blob %s", path); return WGDNA_ERR_TABLES; }
     fseek(f, 0, SEEK_END);
@@ -93,6 +93,7 @@ int tables_load(const char* path, Tables* out, float** d_small, float** d_xwc, f
          put("XVE", S_XVE, NVIB_) && put("XVS", S_XVS, NVIB_) && put("XVMF", S_XVMF, NVIB_ * 9) &&
          put("VIB_LEV", S_VIB, 9);
     std::vector<float> xwc(5 * NWE_ * NWR_), xwt(5 * NWE_ * NWR_);
+    std::vector<float2> xcw(5 * NWE_ * NWR_);
     for (int k = 0; k < 5 && ok; ++k) {
         uint32_t off;
         snprintf(nm, sizeof nm, "XWC%d", k);
@@ -103,15 +104,18 @@ int tables_load(const char* path, Tables* out, float** d_small, float** d_xwc, f
         if (ok) memcpy(xwt.data() + k * NWE_ * NWR_, data + off, 4ull * NWE_ * NWR_);
     }
     if (!ok) { wg_set_error("cross-section blob %s is missing an array", path); return WGDNA_ERR_TABLES; }
+    for (size_t i = 0; i < xcw.size(); ++i) xcw[i] = make_float2(xwc[i], xwt[i]);
+    // guide table: the CDF at breakpoints 0, 16, ..., 240 of every (shell, energy) row
+    for (int k = 0; k < 5; ++k)
+        for (int r = 0; r < NWE_; ++r)
+            for (int m = 0; m < GUIDES; ++m)
+                small[S_GUIDE + (k * NWE_ + r) * GUIDES + m] = xwc[(size_t)k * NWE_ * NWR_ + r * NWR_ + 16 * m];
     WG_CUDA_OK(cudaMalloc(d_small, small.size() * 4));
-    WG_CUDA_OK(cudaMalloc(d_xwc, xwc.size() * 4));
-    WG_CUDA_OK(cudaMalloc(d_xwt, xwt.size() * 4));
+    WG_CUDA_OK(cudaMalloc(d_xcw, xcw.size() * sizeof(float2)));
     WG_CUDA_OK(cudaMemcpy(*d_small, small.data(), small.size() * 4, cudaMemcpyHostToDevice));
-    WG_CUDA_OK(cudaMemcpy(*d_xwc, xwc.data(), xwc.size() * 4, cudaMemcpyHostToDevice));
-    WG_CUDA_OK(cudaMemcpy(*d_xwt, xwt.data(), xwt.size() * 4, cudaMemcpyHostToDevice));
+    WG_CUDA_OK(cudaMemcpy(*d_xcw, xcw.data(), xcw.size() * sizeof(float2), cudaMemcpyHostToDevice));
     t.small = *d_small;
-    t.xwc = *d_xwc;
-    t.xwt = *d_xwt;
+    t.xcw = *d_xcw;
     *out = t;
     return WGDNA_OK;
 }

@@ -30,8 +30,17 @@ constexpr int TW = TB / 32;        // warps per block
 constexpr int STG = 192;           // staged rad entries per warp
 constexpr int STG_FLUSH = 96;      // 32 lanes x at most 3 entries per step
 constexpr uint32_t PRIM_TAKE = 2;  // primaries a warp may start per iteration
-constexpr uint32_t IDLE_LIMIT = 1u << 24;
-constexpr uint32_t READY_LIMIT = 1u << 24;
+constexpr int STASH = 48;          // secondaries a warp keeps in shared memory
+constexpr int STASH_KEEP = 16;     // kept when a full stash spills to the global queue
+constexpr int STASH_SPILL = 32;
+constexpr unsigned long long IDLE_LIMIT_NS = 30000000000ull;   // 30 s without work
+constexpr unsigned long long READY_LIMIT_NS = 2000000000ull;   // 2 s for a queued record
+
+__device__ __forceinline__ unsigned long long gtime() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 
 __constant__ float c_SB[5] = {10.79f, 13.39f, 16.05f, 32.30f, 539.0f};
@@ -47,7 +56,7 @@ constexpr float PI_F = 3.14159265f;
 // counters inside the block's shared block: [0..7] counters, [8..15] sec_stats, [16..23] dbg
 enum { C_OH = 0, C_EAQ = 1, C_H = 2, C_H3O = 3, C_DNA = 4, C_H2 = 5,
        SS_CUT = 9, SS_BOUNDS = 10, SS_STEPS = 11, SS_TERT = 12,
-       D_IONS = 16, D_EXC = 17, D_ESC = 18, D_PRIM = 19, D_WSUM = 20, D_DEPOSITS = 21 };
+       D_IONS = 16, D_EXC = 17, D_ESC = 18, D_PRIM = 19, D_WSUM = 20, C_SECN = 22 };
 
 struct Particle {
     float px, py, pz, E, dx, dy, dz;
@@ -60,10 +69,12 @@ struct Particle {
 
 struct Blk {
     const float* T;       // tables in shared memory
-    float4* srad;         // this warp's staging
+    float4* srad;         // this warp's rad_buf staging
     unsigned long long* skey;
     int* sn;
     uint32_t* cnt;        // block counters
+    StashRec* stash;      // this warp's secondaries
+    int* stn;
 };
 
 __device__ __forceinline__ uint32_t rn(Particle& q, uint32_t k0, uint32_t k1) {
@@ -216,28 +227,53 @@ __device__ __forceinline__ void rotate(float& dx, float& dy, float& dz, float ct
 }
 
 // Born differential CDF: the reference scans breakpoints linearly
-// (helpers.wgsl:98-105) for the last j in [0, N_WR-2] whose prefix is <= r;
-// every committed CDF row is non-decreasing, so a binary search for the first
-// breakpoint > r gives the same index.
+// (helpers.wgsl:98-105) for the last j in [0, N_WR-2] whose prefix is <= r.
+// Every committed CDF row is non-decreasing, so the index is
+// (number of breakpoints <= r) - 1: a guide table in shared memory (every 16th
+// breakpoint) picks the 16-wide window, whose (CDF, energy) pairs are then
+// fetched together with independent loads.
 __device__ __forceinline__ float sample_W_sec(const TArgs& A, const float* T, float E, uint32_t shell, float r) {
     uint32_t lo = 0, hi = NWE_ - 1;                              // helpers.wgsl:88-96
     while (hi - lo > 1u) { uint32_t mid = (lo + hi) / 2u; if (T[S_XWE + mid] <= E) lo = mid; else hi = mid; }
     uint32_t iE = (fabsf(T[S_XWE + hi] - E) < fabsf(T[S_XWE + lo] - E)) ? hi : lo;
-    const float* Cc = A.tab.xwc + shell * (NWE_ * NWR_) + iE * NWR_;
-    const float* Wt = A.tab.xwt + shell * (NWE_ * NWR_) + iE * NWR_;
-    int first = 0, n = NWR_ - 1;
-    while (n > 0) {
-        int half = n >> 1;
-        int mid = first + half;
-        if (__ldg(Cc + mid) <= r) { first = mid + 1; n -= half + 1; } else n = half;
+    const float* G = T + S_GUIDE + (shell * NWE_ + iE) * GUIDES;
+    int M = 0;
+#pragma unroll
+    for (int m = 0; m < GUIDES; ++m) M += (G[m] <= r) ? 1 : 0;
+    int base = 16 * (M - 1);
+    const float2* row = A.tab.xcw + (size_t)(shell * NWE_ + iE) * NWR_;
+    int cnt = 0;
+#pragma unroll
+    for (int k = 1; k <= 16; ++k) {
+        int idx = base + k;
+        if (idx <= NWR_ - 2) cnt += (__ldg(row + idx).x <= r) ? 1 : 0;
     }
-    uint32_t jlo = first > 0 ? (uint32_t)(first - 1) : 0u;
+    uint32_t jlo = (uint32_t)(base + cnt);
     uint32_t jhi = jlo + 1 < NWR_ - 1 ? jlo + 1 : NWR_ - 1;
-    float c0 = __ldg(Cc + jlo), c1 = __ldg(Cc + jhi);
-    float e0 = __ldg(Wt + jlo), e1 = __ldg(Wt + jhi);
+    float2 a = __ldg(row + jlo), b = __ldg(row + jhi);
+    float c0 = a.x, c1 = b.x, e0 = a.y, e1 = b.y;
     if (c1 <= c0) return e0;
     float f = fminf(fmaxf((r - c0) / (c1 - c0), 0.0f), 1.0f);
     return e0 + (e1 - e0) * f;
+}
+
+// Append n stash records to the global queue (one atomic for the batch); the
+// consumer spins on the epoch flag written after the payload.  Records beyond
+// the queue capacity are dropped and counted, as sec_dropped in the reference.
+__device__ void push_global(const TArgs& A, const StashRec* r, int n, int lane_stride) {
+    (void)lane_stride;
+    unsigned long long base = atomicAdd(&A.st->sec_qtail.v, (uint32_t)n);
+    for (int k = 0; k < n; ++k) {
+        unsigned long long slot = base + k;
+        if (slot >= A.max_sec) { atomicAdd(&A.st->sec_drop, 1u); continue; }
+        SecRec* rec = A.secq + slot;
+        rec->pe = make_float4(r[k].x, r[k].y, r[k].z, r[k].E);
+        rec->dir = make_float4(r[k].dx, r[k].dy, r[k].dz, 0.0f);
+        rec->meta.x = r[k].pid;
+        rec->meta.y = r[k].sub;
+        __threadfence();
+        *(volatile uint32_t*)&rec->meta.z = A.epoch;     // publish
+    }
 }
 
 struct XS {
@@ -318,9 +354,9 @@ __device__ __forceinline__ void interact(const TArgs& A, Blk& b, Particle& q, do
                     }
                 }
                 if (W_sec > A.ce) {                              // primary.wgsl:362-413
-                    uint32_t sec_idx = atomicAdd(&A.st->sec_tail, 1u);
+                    atomicAdd(&b.cnt[C_SECN], 1u);
                     q.nsec++;
-                    if (sec_idx < A.max_sec) {
+                    {
                         float E_before = E + bind + W_sec;
                         float cos_s;
                         if (W_sec < 50.0f) {
@@ -344,16 +380,10 @@ __device__ __forceinline__ void interact(const TArgs& A, Blk& b, Particle& q, do
                         float pfl = sqrtf(pfx * pfx + pfy * pfy + pfz * pfz);
                         if (pfl > 1e-10f) { q.dx = pfx / pfl; q.dy = pfy / pfl; q.dz = pfz / pfl; }
                         if (q.nsec >= (1u << 17)) atomicOr(&A.st->err, DERR_KEY_RANGE);
-                        atomicAdd(&A.st->live, 1);
-                        SecRec* rec = A.secq + sec_idx;
-                        rec->pe = make_float4(px, py, pz, W_sec);
-                        rec->dir = make_float4(sdx, sdy, sdz, 0.0f);
-                        rec->meta.x = q.pid;
-                        rec->meta.y = q.nsec;
-                        __threadfence();
-                        *(volatile uint32_t*)&rec->meta.z = A.epoch;     // publish
-                    } else {
-                        atomicAdd(&A.st->sec_drop, 1u);
+                        StashRec r{px, py, pz, W_sec, sdx, sdy, sdz, q.pid, q.nsec};
+                        int slot = atomicAdd(b.stn, 1);
+                        if (slot < STASH) b.stash[slot] = r;
+                        else push_global(A, &r, 1, 0);
                     }
                 }
             } else {
@@ -554,7 +584,6 @@ __device__ __forceinline__ void finish_primary(const TArgs& A, Blk& b, Particle&
     r[1] = make_float4(__uint_as_float(q.nexc), __uint_as_float(esc), q.maxr, 0.0f);
     atomicAdd(&b.cnt[D_IONS], q.nion); atomicAdd(&b.cnt[D_EXC], q.nexc);
     atomicAdd(&b.cnt[D_ESC], esc); atomicAdd(&b.cnt[D_PRIM], 1u);
-    atomicSub(&A.st->live, 1);
     q.active = false;
 }
 
@@ -578,7 +607,7 @@ __device__ __forceinline__ void lane_step(const TArgs& A, Blk& b, Particle& q, d
         interact(A, b, q, dep, x);
         q.it++;
     } else {
-        if (q.it >= A.sec_steps) { atomicSub(&A.st->live, 1); q.active = false; return; }
+        if (q.it >= A.sec_steps) { q.active = false; return; }
         if (q.E < A.ce) {                                        // secondary.wgsl:100-124
             deposit(A, dep, q.px, q.py, q.pz, q.E);
             atomicAdd(&b.cnt[C_EAQ], 1u);
@@ -590,18 +619,16 @@ __device__ __forceinline__ void lane_step(const TArgs& A, Blk& b, Particle& q, d
             }
             put(A, b, q, epx, epy, epz, 5.0f);
             atomicAdd(&b.cnt[SS_CUT], 1u);
-            atomicSub(&A.st->live, 1);
             q.active = false;
             return;
         }
         if (fabsf(q.px) >= box || fabsf(q.py) >= box || fabsf(q.pz) >= box) {
             atomicAdd(&b.cnt[SS_BOUNDS], 1u);
-            atomicSub(&A.st->live, 1);
             q.active = false;
             return;
         }
         XS x; float dist;
-        if (!fly(A, b, q, x, dist)) { atomicSub(&A.st->live, 1); q.active = false; return; }
+        if (!fly(A, b, q, x, dist)) { q.active = false; return; }
         nsteps++;
         atomicAdd(&b.cnt[SS_STEPS], 1u);
         interact(A, b, q, dep, x);
@@ -614,7 +641,7 @@ __device__ __forceinline__ void flush_staging(const TArgs& A, Blk& b, int lane) 
     int n = *b.sn;
     if (n == 0) return;
     unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(&A.st->rad_next, (unsigned long long)n);
+    if (lane == 0) base = atomicAdd(&A.st->rad_next.v, (unsigned long long)n);
     base = __shfl_sync(0xffffffffu, base, 0);
     int ndrop = 0;
     for (int i = lane; i < n; i += 32) {
@@ -628,40 +655,66 @@ __device__ __forceinline__ void flush_staging(const TArgs& A, Blk& b, int lane) 
     __syncwarp();
 }
 
+__device__ __forceinline__ void load_secondary(Particle& q, const StashRec& r) {
+    q.px = r.x; q.py = r.y; q.pz = r.z; q.E = r.E;
+    q.dx = r.dx; q.dy = r.dy; q.dz = r.dz;
+    q.pid = r.pid; q.sub = r.sub; q.seq = 0; q.it = 0; q.nsec = 0;
+    q.blk = 0; q.ri = 4; q.prim = false; q.active = true;
+}
+
 __global__ void __launch_bounds__(TB, 2) k_transport(TArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     float* T = reinterpret_cast<float*>(smem);
     float4* stg_rad = reinterpret_cast<float4*>(smem + S_TOTAL_PAD * 4);
     unsigned long long* stg_key = reinterpret_cast<unsigned long long*>(stg_rad + TW * STG);
-    int* stg_n = reinterpret_cast<int*>(stg_key + TW * STG);
-    uint32_t* cnt = reinterpret_cast<uint32_t*>(stg_n + TW);
+    StashRec* stash = reinterpret_cast<StashRec*>(stg_key + TW * STG);
+    int* stg_n = reinterpret_cast<int*>(stash + TW * STASH);
+    int* stn = stg_n + TW;
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(stn + TW);
     for (int i = threadIdx.x; i < S_TOTAL; i += TB) T[i] = A.tab.small[i];
-    if (threadIdx.x < TW) stg_n[threadIdx.x] = 0;
+    if (threadIdx.x < TW) { stg_n[threadIdx.x] = 0; stn[threadIdx.x] = 0; }
     if (threadIdx.x < 24) cnt[threadIdx.x] = 0;
     __syncthreads();
 
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    Blk b{T, stg_rad + w * STG, stg_key + w * STG, stg_n + w, cnt};
+    Blk b{T, stg_rad + w * STG, stg_key + w * STG, stg_n + w, cnt, stash + w * STASH, stn + w};
     DevState* S = A.st;
     Particle q;
     q.active = false;
     double dep = 0.0;
     unsigned long long nsteps = 0;
-    uint32_t idle = 0;
+    bool busy = false;
+    unsigned sleep_ns = 64;
+    unsigned long long idle_since = 0;
 
-    for (;;) {
+    for (uint32_t it = 0;; ++it) {
         unsigned need = __ballot_sync(0xffffffffu, !q.active);
+        // 1) this warp's stash (LIFO)
         if (need) {
-            // 1) queued secondaries
+            int sn = *(volatile int*)b.stn;
+            if (sn > 0) {
+                uint32_t take = min((uint32_t)__popc(need), (uint32_t)sn);
+                uint32_t rank = __popc(need & lt);
+                if (!q.active && rank < take) load_secondary(q, b.stash[sn - 1 - rank]);
+                __syncwarp();
+                if (lane == 0) *b.stn = sn - (int)take;
+                __syncwarp();
+                need = __ballot_sync(0xffffffffu, !q.active);
+            }
+        }
+        const bool idle_warp = need == 0xffffffffu;
+        const bool poll = idle_warp || (it & 7u) == 0u;
+        // 2) the global queue
+        if (need && poll) {
             uint32_t base = 0, got = 0;
             if (lane == 0) {
-                uint32_t lim = min(*(volatile uint32_t*)&S->sec_tail, A.max_sec);
-                uint32_t h = *(volatile uint32_t*)&S->sec_head;
+                uint32_t lim = min(*(volatile uint32_t*)&S->sec_qtail.v, A.max_sec);
+                uint32_t h = *(volatile uint32_t*)&S->sec_head.v;
                 uint32_t k = __popc(need);
                 while (h < lim) {
                     uint32_t take = min(k, lim - h);
-                    uint32_t old = atomicCAS(&S->sec_head, h, h + take);
+                    uint32_t old = atomicCAS(&S->sec_head.v, h, h + take);
                     if (old == h) { base = h; got = take; break; }
                     h = old;
                 }
@@ -671,64 +724,73 @@ __global__ void __launch_bounds__(TB, 2) k_transport(TArgs A) {
             uint32_t rank = __popc(need & lt);
             if (!q.active && rank < got) {
                 const SecRec* rec = A.secq + base + rank;
-                uint32_t spins = 0;
+                unsigned long long t0 = gtime();
+                bool ok = true;
                 while (*(volatile const uint32_t*)&rec->meta.z != A.epoch) {
-                    if (++spins > READY_LIMIT) { atomicOr(&S->err, DERR_QUEUE_WAIT); break; }
+                    if (gtime() - t0 > READY_LIMIT_NS) { atomicOr(&S->err, DERR_QUEUE_WAIT); ok = false; break; }
                     __nanosleep(64);
                 }
                 __threadfence();
-                if (spins <= READY_LIMIT) {
+                if (ok) {
                     float4 pe = __ldcg(&rec->pe);
                     float4 dr = __ldcg(&rec->dir);
                     uint4 mt = __ldcg(&rec->meta);
-                    q.px = pe.x; q.py = pe.y; q.pz = pe.z; q.E = pe.w;
-                    q.dx = dr.x; q.dy = dr.y; q.dz = dr.z;
-                    q.pid = mt.x; q.sub = mt.y; q.seq = 0; q.it = 0; q.nsec = 0;
-                    q.blk = 0; q.ri = 4; q.prim = false; q.active = true;
-                } else {
-                    atomicSub(&S->live, 1);
+                    StashRec r{pe.x, pe.y, pe.z, pe.w, dr.x, dr.y, dr.z, mt.x, mt.y};
+                    load_secondary(q, r);
                 }
             }
-            // 2) new primaries
             need = __ballot_sync(0xffffffffu, !q.active);
-            if (need && *(volatile uint32_t*)&S->prim_next < A.np) {
-                uint32_t pb = 0, pg = 0;
-                if (lane == 0) {
-                    uint32_t take = min((uint32_t)__popc(need), PRIM_TAKE);
-                    uint32_t old = atomicAdd(&S->prim_next, take);
-                    if (old < A.np) {
-                        pg = min(take, A.np - old);
-                        pb = old;
-                        atomicAdd(&S->live, (int)pg);
-                    }
-                }
-                pb = __shfl_sync(0xffffffffu, pb, 0);
-                pg = __shfl_sync(0xffffffffu, pg, 0);
-                uint32_t r2 = __popc(need & lt);
-                if (!q.active && r2 < pg) start_primary(A, q, pb + r2);
+        }
+        // 3) new primaries
+        if (need && poll && *(volatile uint32_t*)&S->prim_next.v < A.np) {
+            uint32_t pb = 0, pg = 0;
+            if (lane == 0) {
+                uint32_t take = min((uint32_t)__popc(need), PRIM_TAKE);
+                uint32_t old = atomicAdd(&S->prim_next.v, take);
+                if (old < A.np) { pg = min(take, A.np - old); pb = old; }
             }
+            pb = __shfl_sync(0xffffffffu, pb, 0);
+            pg = __shfl_sync(0xffffffffu, pg, 0);
+            uint32_t r2 = __popc(need & lt);
+            if (!q.active && r2 < pg) start_primary(A, q, pb + r2);
         }
         unsigned act = __ballot_sync(0xffffffffu, q.active);
+        if (act && !busy) { busy = true; if (lane == 0) atomicAdd(&S->busy.v, 1u); }
         if (!act) {
+            // no lanes and an empty stash: idle
+            if (busy) { busy = false; if (lane == 0) atomicSub(&S->busy.v, 1u); idle_since = gtime(); }
             int done = 0;
             if (lane == 0) {
-                uint32_t lim = min(*(volatile uint32_t*)&S->sec_tail, A.max_sec);
-                done = *(volatile uint32_t*)&S->prim_next >= A.np &&
-                       *(volatile uint32_t*)&S->sec_head >= lim && *(volatile int*)&S->live <= 0;
+                uint32_t lim = min(*(volatile uint32_t*)&S->sec_qtail.v, A.max_sec);
+                done = *(volatile uint32_t*)&S->prim_next.v >= A.np &&
+                       *(volatile uint32_t*)&S->sec_head.v >= lim && *(volatile uint32_t*)&S->busy.v == 0u;
             }
             done = __shfl_sync(0xffffffffu, done, 0);
             if (done) break;
-            if (++idle > IDLE_LIMIT) { if (lane == 0) atomicOr(&S->err, DERR_IDLE_WAIT); break; }
-            __nanosleep(256);
+            if (idle_since == 0) idle_since = gtime();
+            if (gtime() - idle_since > IDLE_LIMIT_NS) { if (lane == 0) atomicOr(&S->err, DERR_IDLE_WAIT); break; }
+            __nanosleep(sleep_ns);
+            sleep_ns = min(sleep_ns * 2, 8192u);
             continue;
         }
-        idle = 0;
+        sleep_ns = 64;
+        idle_since = 0;
         if (q.active) lane_step(A, b, q, dep, nsteps);
+        __syncwarp();
+        // stash overflow went straight to the global queue; spill a full stash
+        if (lane == 0) {
+            int sn = *b.stn;
+            if (sn > STASH) sn = STASH;
+            if (sn >= STASH_SPILL) {
+                push_global(A, b.stash + STASH_KEEP, sn - STASH_KEEP, 0);
+                sn = STASH_KEEP;
+            }
+            *b.stn = sn;
+        }
         __syncwarp();
         if (*b.sn >= STG_FLUSH) flush_staging(A, b, lane);
     }
     flush_staging(A, b, lane);
-    // per-lane sums -> warp -> global
     for (int o = 16; o; o >>= 1) {
         dep += __shfl_xor_sync(0xffffffffu, dep, o);
         nsteps += __shfl_xor_sync(0xffffffffu, nsteps, o);
@@ -739,9 +801,11 @@ __global__ void __launch_bounds__(TB, 2) k_transport(TArgs A) {
     }
     __syncthreads();
     if (threadIdx.x < 24 && cnt[threadIdx.x]) {
-        uint32_t* g = threadIdx.x < 8 ? &S->counters[threadIdx.x]
-                     : threadIdx.x < 16 ? &S->sec_stats[threadIdx.x - 8] : &S->dbg[threadIdx.x - 16];
-        atomicAdd(g, cnt[threadIdx.x]);
+        uint32_t v = cnt[threadIdx.x];
+        if (threadIdx.x == C_SECN) atomicAdd(&S->sec_tail.v, v);
+        else if (threadIdx.x < 8) atomicAdd(&S->counters[threadIdx.x], v);
+        else if (threadIdx.x < 16) atomicAdd(&S->sec_stats[threadIdx.x - 8], v);
+        else atomicAdd(&S->dbg[threadIdx.x - 16], v);
     }
 }
 
@@ -837,7 +901,7 @@ __global__ void k_reduce(const float* results, uint32_t np, const uint32_t* dose
 
 // ------------------------------------------------------------------ host side
 size_t transport_smem_bytes() {
-    return S_TOTAL_PAD * 4 + TW * STG * 16 + TW * STG * 8 + TW * 4 + 24 * 4;
+    return S_TOTAL_PAD * 4 + TW * STG * 16 + TW * STG * 8 + TW * STASH * sizeof(StashRec) + 2 * TW * 4 + 24 * 4;
 }
 
 int transport_blocks(int device) {
