@@ -155,6 +155,25 @@ int wgdna_cluster_dsb(wgdna_ctx *ctx, const uint8_t *hits, wgdna_dsb_result *out
  * (app.ts:182-185 with the worker backend, where indirect scoring is skipped). */
 int wgdna_score(wgdna_ctx *ctx, uint32_t lcg_state, wgdna_ssb_result *ssb, wgdna_dsb_result *dsb);
 
+/* Direct SSB scoring that allocates nothing.  No counterpart in the reference:
+ * it serves callers that cannot call cudaMalloc (a host running under another
+ * framework's memory pool or a fixed device-memory budget, or code that must
+ * not allocate while a CUDA graph is being captured).  All pointers except
+ * `dna` and `out` are device pointers owned by the caller: d_rad holds rad_n
+ * entries (16-byte aligned), d_fy/d_fz/d_rbb0/d_rbb1 the target built by
+ * wgdna_build_dna_target, and d_hits (4-byte aligned, 2*n_bp bytes rounded up
+ * to a multiple of 4) is OR-ed into.  The scratch is a fixed 16.1 MB device
+ * array that every GPU loading the library holds until exit; at most
+ * 4,194,304 entries per call (larger lists fail with WGDNA_ERR_CAPACITY and
+ * can be split where consecutive entries differ, chaining lcg_state and
+ * hits).  The first call on a device looks up the array's device address, so
+ * make it before any stream capture.  Calls share the array: calls that
+ * overlap on the GPU race.  Runs on cuda_stream (NULL = the default stream)
+ * and returns after the stream reaches the end of the call. */
+int wgdna_score_direct_noalloc(const float *d_rad, uint64_t rad_n, const float *d_fy, const float *d_fz,
+                               const float *d_rbb0, const float *d_rbb1, const wgdna_dna_info *dna,
+                               uint32_t lcg_state, uint8_t *d_hits, void *cuda_stream, wgdna_ssb_result *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,7 +20,8 @@ ERRORS = {-1: "WGDNA_ERR_ARG", -2: "WGDNA_ERR_CUDA", -3: "WGDNA_ERR_TABLES", -4:
 EXPORTS = ["wgdna_default_cfg", "wgdna_create", "wgdna_destroy", "wgdna_last_error", "wgdna_version",
            "wgdna_set_stream", "wgdna_transport", "wgdna_transport_copy_out", "wgdna_run_transport",
            "wgdna_run_irt", "wgdna_irt", "wgdna_build_dna_target", "wgdna_set_dna_target",
-           "wgdna_score_direct", "wgdna_score_indirect", "wgdna_cluster_dsb", "wgdna_score"]
+           "wgdna_score_direct", "wgdna_score_indirect", "wgdna_cluster_dsb", "wgdna_score",
+           "wgdna_score_direct_noalloc"]
 
 
 class WgdnaError(RuntimeError):
@@ -106,6 +107,8 @@ def lib():
         "wgdna_score_indirect": (C.c_int, [vp, vp, vp, C.c_uint64, C.c_uint32, vp, P(SsbResult)]),
         "wgdna_cluster_dsb": (C.c_int, [vp, vp, P(DsbResult)]),
         "wgdna_score": (C.c_int, [vp, C.c_uint32, P(SsbResult), P(DsbResult)]),
+        "wgdna_score_direct_noalloc": (C.c_int, [vp, C.c_uint64, vp, vp, vp, vp, P(DnaInfo), C.c_uint32, vp, vp,
+                                                 P(SsbResult)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
