@@ -115,6 +115,10 @@ int wgdna_run_irt(wgdna_ctx *ctx, const float *rad_buf, uint64_t rad_n, uint32_t
                   double E_eV, uint64_t seed, wgdna_irt_result *out);
 /* The same on the rad_buf left in device memory by the last wgdna_transport. */
 int wgdna_irt(wgdna_ctx *ctx, uint32_t n_therm, double E_eV, uint64_t seed, wgdna_irt_result *out);
+/* Per-reaction constants of the 9-reaction table (irt-worker.js:240-279), host
+ * only: out[r] = {sigma, sigma_eff, rc, kdif, kact, prob} in nm / nm^3 ns^-1;
+ * the worker reports sigma and rc in its rxn_info (irt-worker.js:690-694). */
+int wgdna_reaction_table(double out[9][6]);
 
 /* ---------------------------------------------------------------- scoring */
 typedef struct {

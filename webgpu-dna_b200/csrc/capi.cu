@@ -470,6 +470,7 @@ static void irt_constants(IrtConst* C) {
             else { se = -rc / (1 - exp(rc / sc)); kd = 4 * M_PI * Ds * se; if (self) kd /= 2; }
             C->sigma_eff[r] = se; C->kdif[r] = kd;
             double ka = kd * k / (kd - k);
+            C->kact[r] = ka;
             C->prob[r] = Rs / (Rs + (kd / ka) * (se + Rs));
             C->acc_s[r] = rc == 0 ? sc : se;
             C->acc_c[r] = k / kd;
@@ -666,4 +667,15 @@ extern "C" int wgdna_score(wgdna_ctx* c, uint32_t lcg_state, wgdna_ssb_result* s
     TRY(hits_in(c, nullptr));
     TRY(score_dev(c, c->d_rad, nullptr, c->last_rad_n, 0.15, 1, lcg_state, ssb));
     return cluster_dev(c, dsb);
+}
+
+extern "C" int wgdna_reaction_table(double out[9][6]) {
+    if (!out) { wg_set_error("wgdna_reaction_table: NULL argument"); return WGDNA_ERR_ARG; }
+    IrtConst C;
+    irt_constants(&C);
+    for (int r = 0; r < 9; ++r) {
+        out[r][0] = C.sigma[r]; out[r][1] = C.sigma_eff[r]; out[r][2] = C.rc[r];
+        out[r][3] = C.kdif[r]; out[r][4] = C.kact[r]; out[r][5] = C.prob[r];
+    }
+    return WGDNA_OK;
 }

@@ -7,6 +7,7 @@ namespace wg {
 struct IrtConst {
     double sigma[9], sigma_eff[9], rc[9], kdif[9], kobs[9], prob[9], a_pdc[9], coth_sig[9];
     double acc_s[9], acc_c[9], acc_add[9];   // acceptance-radius bound (irt.cu r_acc)
+    double kact[9];
     int type[9], nprod[9], prod0[9], prod1[9];
     int map[36];
     double D[6];

@@ -21,7 +21,7 @@ EXPORTS = ["wgdna_default_cfg", "wgdna_create", "wgdna_destroy", "wgdna_last_err
            "wgdna_set_stream", "wgdna_transport", "wgdna_transport_copy_out", "wgdna_run_transport",
            "wgdna_run_irt", "wgdna_irt", "wgdna_build_dna_target", "wgdna_set_dna_target",
            "wgdna_score_direct", "wgdna_score_indirect", "wgdna_cluster_dsb", "wgdna_score",
-           "wgdna_score_direct_noalloc"]
+           "wgdna_score_direct_noalloc", "wgdna_reaction_table"]
 
 
 class WgdnaError(RuntimeError):
@@ -107,6 +107,7 @@ def lib():
         "wgdna_score_indirect": (C.c_int, [vp, vp, vp, C.c_uint64, C.c_uint32, vp, P(SsbResult)]),
         "wgdna_cluster_dsb": (C.c_int, [vp, vp, P(DsbResult)]),
         "wgdna_score": (C.c_int, [vp, C.c_uint32, P(SsbResult), P(DsbResult)]),
+        "wgdna_reaction_table": (C.c_int, [vp]),
         "wgdna_score_direct_noalloc": (C.c_int, [vp, C.c_uint64, vp, vp, vp, vp, P(DnaInfo), C.c_uint32, vp, vp,
                                                  P(SsbResult)]),
     }
@@ -169,3 +170,11 @@ class Context:
 
     def set_stream(self, stream_ptr):
         check("wgdna_set_stream", lib().wgdna_set_stream(self.h, C.c_void_p(stream_ptr or 0)))
+
+
+def reaction_table():
+    """Per-reaction constants (irt-worker.js:240-279) as a (9, 6) array:
+    sigma, sigma_eff, rc, kdif, kact, prob."""
+    out = np.zeros((9, 6), np.float64)
+    check("wgdna_reaction_table", lib().wgdna_reaction_table(ptr(out)))
+    return out

@@ -14,7 +14,9 @@ def _chem_result(r, rad_n, log=None):
         g = r.G[c]
         timeline.append({"label": CHECKPOINT_LABELS[c], "t_ns": CHECKPOINTS_NS[c], "G_OH": g[0], "G_eaq": g[1],
                          "G_H": g[2], "G_H2O2": g[3], "G_H2": g[4]})
-    rxn_info = [{"label": IRT_WORKER_RXN_LABELS[k], "count": int(r.rxn_counts[k])} for k in range(9)]
+    tab = _lib.reaction_table()
+    rxn_info = [{"label": IRT_WORKER_RXN_LABELS[k], "count": int(r.rxn_counts[k]),
+                 "sigma": f"{tab[k, 0]:.4f}", "rc": f"{tab[k, 2]:.3f}"} for k in range(9)]
     res = {"chem_n": int(rad_n), "t_wall": float(r.ms), "timeline": timeline, "chem_pos_final": None,
            "chem_alive_final": None, "n_reacted": int(r.n_reacted), "rxn_info": rxn_info,
            "n_tracks": int(r.n_tracks), "n_pairs": int(r.n_pairs), "n_events": int(r.n_events),
