@@ -70,6 +70,7 @@ struct wgdna_ctx {
     double *d_px = nullptr, *d_py = nullptr, *d_pz = nullptr, *d_tb = nullptr;
     int8_t* d_sp = nullptr;
     uint8_t* d_alive8 = nullptr;
+    uint16_t *d_lst = nullptr, *d_lpos = nullptr;
     double* d_evt = nullptr;
     uint32_t* d_evab = nullptr;
     uint32_t* d_track_next = nullptr;
@@ -182,7 +183,7 @@ extern "C" void wgdna_destroy(wgdna_ctx* c) {
                     c->d_perm, c->d_secq, c->d_st, c->d_Eprim, c->d_pid_cnt, c->d_pid_off, c->d_pid_cur,
                     c->d_red, c->d_err, c->d_fy, c->d_fz, c->d_rbb0, c->d_rbb1, c->d_hits, c->d_alive,
                     c->sc.info, c->sc.last_brk, c->sc.cnt0, c->sc.cnt1, c->sc.cs_in, c->sc.base, c->sc.u64,
-                    c->sc.fib, c->d_px, c->d_py, c->d_pz, c->d_tb, c->d_sp, c->d_alive8, c->d_evt, c->d_evab,
+                    c->sc.fib, c->d_px, c->d_py, c->d_pz, c->d_tb, c->d_sp, c->d_alive8, c->d_lst, c->d_lpos, c->d_evt, c->d_evab,
                     c->d_track_next, c->d_acc_tl, c->d_acc, c->d_maxpid};
     for (void* p : ptrs) if (p) cudaFree(p);
     for (auto& ev : c->ev) if (ev) cudaEventDestroy(ev);
@@ -213,6 +214,7 @@ static IArgs make_iargs(wgdna_ctx* c, uint32_t nseg, uint64_t seed) {
     a.k0 = (uint32_t)seed; a.k1 = (uint32_t)(seed >> 32);
     a.cap = c->irt_cap; a.ecap = c->irt_ecap; a.nwarps = c->irt_warps;
     a.px = c->d_px; a.py = c->d_py; a.pz = c->d_pz; a.tb = c->d_tb; a.sp = c->d_sp; a.alive = c->d_alive8;
+    a.lst = c->d_lst; a.lpos = c->d_lpos;
     a.ev_t = c->d_evt; a.ev_ab = c->d_evab; a.track_next = c->d_track_next;
     a.acc_tl = c->d_acc_tl; a.acc = c->d_acc; a.err = c->d_err;
     return a;
@@ -335,6 +337,7 @@ static int irt_ensure(wgdna_ctx* c, uint32_t cap) {
     size_t nn = (size_t)warps * cap, ne = (size_t)warps * 2 * ecap;
     TRY(dalloc(&c->d_px, nn)); TRY(dalloc(&c->d_py, nn)); TRY(dalloc(&c->d_pz, nn)); TRY(dalloc(&c->d_tb, nn));
     TRY(dalloc(&c->d_sp, nn)); TRY(dalloc(&c->d_alive8, nn));
+    TRY(dalloc(&c->d_lst, 6 * nn)); TRY(dalloc(&c->d_lpos, nn));
     TRY(dalloc(&c->d_evt, ne)); TRY(dalloc(&c->d_evab, ne));
     if (!c->d_track_next) TRY(dalloc(&c->d_track_next, 1));
     if (!c->d_acc_tl) TRY(dalloc(&c->d_acc_tl, 35));

@@ -88,9 +88,17 @@ __device__ double pdc_warp(uint32_t i, uint32_t j, uint32_t pid, uint32_t k0, ui
             if (U < p / (p + q * M)) { double h = U * (p + q * M) / 2; X = h * h; }
             else { double h = 2 / ((1 - U) * (p + q * M) / M); X = h * h; }
             U = u01d(w.z, w.w);
-            double sqX = sqrt(X);
-            double lambdax = exp_(-b * b / X) * (1.0 - a * sqrt(3.141592653589793 * X) * erfcx_(b / sqX + a * sqX));
-            ok = (X <= 2.0 * b / a && U <= lambdax) || (X >= 2.0 * b / a && U * M / X <= lambdax);
+            // lambdax = e * (1 - a sqrt(pi X) erfcx(.)) with a second factor <= 1, so its
+            // computed value never exceeds e: a trial that fails against e alone is
+            // rejected without evaluating erfcx (same decision as the full test)
+            double e = exp_(-b * b / X);
+            double t2 = 2.0 * b / a;
+            double v = U * M / X;
+            if ((X <= t2 && U <= e) || (X >= t2 && v <= e)) {
+                double sqX = sqrt(X);
+                double lambdax = e * (1.0 - a * sqrt(3.141592653589793 * X) * erfcx_(b / sqX + a * sqX));
+                ok = (X <= t2 && U <= lambdax) || (X >= t2 && v <= lambdax);
+            }
         }
         unsigned m = __ballot_sync(0xffffffffu, ok);
         if (m) return __shfl_sync(0xffffffffu, X, __ffs(m) - 1);
@@ -224,6 +232,7 @@ __global__ void __launch_bounds__(IB) k_irt(IArgs A) {
     __shared__ uint32_t s_hab[IB / 32][HS];
     __shared__ IrtConst s_c;
     __shared__ uint32_t s_row[6];
+    __shared__ int s_lc[IB / 32][6];
     for (int k = threadIdx.x; k < (int)(sizeof(IrtConst) / 4); k += IB)
         reinterpret_cast<uint32_t*>(&s_c)[k] = reinterpret_cast<const uint32_t*>(&c_irt)[k];
     __syncthreads();
@@ -244,6 +253,9 @@ __global__ void __launch_bounds__(IB) k_irt(IArgs A) {
     double* tb = A.tb + (size_t)gw * A.cap;
     int8_t* sp = A.sp + (size_t)gw * A.cap;
     uint8_t* alive = A.alive + (size_t)gw * A.cap;
+    uint16_t* lst = A.lst + (size_t)gw * 6 * A.cap;
+    uint16_t* lpos = A.lpos + (size_t)gw * A.cap;
+    int* lc = s_lc[wl];
     double* ET = A.ev_t + (size_t)gw * 2 * A.ecap;          // [0, ecap): initial events
     uint32_t* EAB = A.ev_ab + (size_t)gw * 2 * A.ecap;
     Heap H{s_ht[wl], s_hab[wl], ET + A.ecap, EAB + A.ecap};  // product events
@@ -313,8 +325,18 @@ __global__ void __launch_bounds__(IB) k_irt(IArgs A) {
         for (uint32_t c = 0; c < n; c += 32) {
             uint32_t k = c + lane;
             int spc = k < n ? sp[k] : -1;
-            for (int q = 0; q < 6; ++q) cnt[q] += __popc(__ballot_sync(FULL, spc == q));
+            for (int q = 0; q < 6; ++q) {
+                unsigned m = __ballot_sync(FULL, spc == q);
+                if (spc == q) {
+                    uint32_t at = cnt[q] + __popc(m & lt);
+                    lst[q * A.cap + at] = (uint16_t)k;
+                    lpos[k] = (uint16_t)at;
+                }
+                cnt[q] += __popc(m);
+            }
         }
+        if (lane < 6) lc[lane] = (int)cnt[lane];
+        __syncwarp();
         // -------------------------------------------------- initial pairing (:539-558)
         uint32_t nev = 0;
         bool ev_over = false;
@@ -425,6 +447,14 @@ __global__ void __launch_bounds__(IB) k_irt(IArgs A) {
                         valid = 1;
                         alive[ei] = 0; alive[ej] = 0;
                         cnt[si]--; cnt[sj]--;
+                        for (int w2 = 0; w2 < 2; ++w2) {
+                            int k = w2 == 0 ? ei : ej, q = w2 == 0 ? si : sj;
+                            uint32_t at = lpos[k];
+                            uint16_t last = lst[q * A.cap + lc[q] - 1];
+                            lst[q * A.cap + at] = last;
+                            lpos[last] = (uint16_t)at;
+                            lc[q]--;
+                        }
                         n_reacted++;
                         rxn[ri]++;
                         if (ri == 3 || ri == 4 || ri == 6) h2c += 1;
@@ -457,6 +487,9 @@ __global__ void __launch_bounds__(IB) k_irt(IArgs A) {
                     px[id] = nx; py[id] = ny; pz[id] = nz; tb[id] = et;
                     sp[id] = (int8_t)nsp; alive[id] = 1;
                     cnt[nsp]++;
+                    lst[nsp * A.cap + lc[nsp]] = (uint16_t)id;
+                    lpos[id] = (uint16_t)lc[nsp];
+                    lc[nsp]++;
                 }
                 ntot++;
                 __syncwarp();
@@ -464,12 +497,15 @@ __global__ void __launch_bounds__(IB) k_irt(IArgs A) {
                 // pairWithAlive (:430-465)
                 double Di = C.D[nsp];
                 uint32_t rowp = s_row[nsp];
-                for (uint32_t c0 = 0; c0 < ntot; c0 += 32) {
-                    uint32_t jj = c0 + lane;
-                    bool cand = jj < ntot && jj != id && alive[jj];
-                    int s2 = cand ? sp[jj] : 0;
-                    int r2i = (int)((rowp >> (4 * s2)) & 15u);
-                    cand = cand && r2i != 15;
+                // partners: the alive particles of the species that react with nsp
+                for (int s2 = 0; s2 < 6; ++s2) {
+                const int r2i = (int)((rowp >> (4 * s2)) & 15u);
+                if (r2i == 15) continue;
+                const uint32_t len = (uint32_t)lc[s2];
+                for (uint32_t c0 = 0; c0 < len; c0 += 32) {
+                    uint32_t li = c0 + lane;
+                    uint32_t jj = li < len ? lst[s2 * A.cap + li] : 0u;
+                    bool cand = li < len && jj != id;
                     bool acc = false, pdcq = false;
                     double ta = 0, pa = 0, pb = 0, pD = 0;
                     if (cand) {
@@ -532,6 +568,7 @@ __global__ void __launch_bounds__(IB) k_irt(IArgs A) {
                             } else heap_over = true;
                         }
                     }
+                }
                 }
                 __syncwarp();
                 __threadfence_block();

@@ -22,6 +22,8 @@ struct IArgs {
     double *px, *py, *pz, *tb;           // [warp][cap]
     int8_t* sp;
     uint8_t* alive;
+    uint16_t* lst;                       // [warp][6][cap]: alive particles of each species
+    uint16_t* lpos;                      // [warp][cap]: position of a particle in its list
     double* ev_t;                        // [warp][2*ecap]: initial events, then heap overflow
     uint32_t* ev_ab;                     // packed (a << 16) | b
     uint32_t* track_next;
