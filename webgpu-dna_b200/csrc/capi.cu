@@ -66,14 +66,19 @@ struct wgdna_ctx {
     ScoreScratch sc{};
     unsigned long long sc_cap = 0;
     // IRT scratch
-    uint32_t irt_cap = 0, irt_ecap = 0, irt_warps = 0;
+    size_t irt_slots = 0, irt_evslots = 0, irt_hov = 0;
+    uint32_t irt_tracks = 0, irt_hcap = 0;
     double *d_px = nullptr, *d_py = nullptr, *d_pz = nullptr, *d_tb = nullptr;
     int8_t* d_sp = nullptr;
     uint8_t* d_alive8 = nullptr;
     uint16_t *d_lst = nullptr, *d_lpos = nullptr;
     double* d_evt = nullptr;
     uint32_t* d_evab = nullptr;
-    uint32_t* d_track_next = nullptr;
+    double* d_hov_t = nullptr;
+    uint32_t* d_hov_ab = nullptr;
+    uint32_t* d_track = nullptr;          // 10 per track: tn, th2, ttiles, tev, tlc[6]
+    unsigned long long* d_toff = nullptr;
+    uint32_t* d_irt_cnt = nullptr;
     double* d_acc_tl = nullptr;
     unsigned long long* d_acc = nullptr;
     uint32_t* d_maxpid = nullptr;
@@ -184,7 +189,7 @@ extern "C" void wgdna_destroy(wgdna_ctx* c) {
                     c->d_red, c->d_err, c->d_fy, c->d_fz, c->d_rbb0, c->d_rbb1, c->d_hits, c->d_alive,
                     c->sc.info, c->sc.last_brk, c->sc.cnt0, c->sc.cnt1, c->sc.cs_in, c->sc.base, c->sc.u64,
                     c->sc.fib, c->d_px, c->d_py, c->d_pz, c->d_tb, c->d_sp, c->d_alive8, c->d_lst, c->d_lpos, c->d_evt, c->d_evab,
-                    c->d_track_next, c->d_acc_tl, c->d_acc, c->d_maxpid};
+                    c->d_hov_t, c->d_hov_ab, c->d_track, c->d_toff, c->d_irt_cnt, c->d_acc_tl, c->d_acc, c->d_maxpid};
     for (void* p : ptrs) if (p) cudaFree(p);
     for (auto& ev : c->ev) if (ev) cudaEventDestroy(ev);
     if (c->own) cudaStreamDestroy(c->own);
@@ -212,10 +217,15 @@ static IArgs make_iargs(wgdna_ctx* c, uint32_t nseg, uint64_t seed) {
     memset(&a, 0, sizeof a);
     a.rad = c->d_rad; a.seg_off = c->d_pid_off; a.nseg = nseg; a.pid_base = c->irt_pid_base;
     a.k0 = (uint32_t)seed; a.k1 = (uint32_t)(seed >> 32);
-    a.cap = c->irt_cap; a.ecap = c->irt_ecap; a.nwarps = c->irt_warps;
     a.px = c->d_px; a.py = c->d_py; a.pz = c->d_pz; a.tb = c->d_tb; a.sp = c->d_sp; a.alive = c->d_alive8;
     a.lst = c->d_lst; a.lpos = c->d_lpos;
-    a.ev_t = c->d_evt; a.ev_ab = c->d_evab; a.track_next = c->d_track_next;
+    a.ev_t = c->d_evt; a.ev_ab = c->d_evab;
+    const size_t T = c->irt_tracks;
+    a.tn = c->d_track; a.th2 = c->d_track + T; a.ttiles = c->d_track + 2 * T; a.tev = c->d_track + 3 * T;
+    a.tlc = c->d_track + 4 * T;
+    a.toff = c->d_toff;
+    a.hov_t = c->d_hov_t; a.hov_ab = c->d_hov_ab; a.hcap = c->irt_hcap;
+    a.counters = c->d_irt_cnt;
     a.acc_tl = c->d_acc_tl; a.acc = c->d_acc; a.err = c->d_err;
     return a;
 }
@@ -329,20 +339,36 @@ extern "C" int wgdna_run_transport(wgdna_ctx* c, const wgdna_transport_params* p
 // ------------------------------------------------------------------ Phase C
 static void irt_constants(IrtConst* C);
 
-static int irt_ensure(wgdna_ctx* c, uint32_t cap) {
-    int blocks = irt_blocks(c->device);
-    uint32_t warps = (uint32_t)blocks * 4u;
-    uint32_t ecap = cap * 4u + 4096u;     // events per track: ~1.3 per particle at 10 keV
-    if (cap <= c->irt_cap && warps <= c->irt_warps && ecap <= c->irt_ecap) return WGDNA_OK;
-    size_t nn = (size_t)warps * cap, ne = (size_t)warps * 2 * ecap;
-    TRY(dalloc(&c->d_px, nn)); TRY(dalloc(&c->d_py, nn)); TRY(dalloc(&c->d_pz, nn)); TRY(dalloc(&c->d_tb, nn));
-    TRY(dalloc(&c->d_sp, nn)); TRY(dalloc(&c->d_alive8, nn));
-    TRY(dalloc(&c->d_lst, 6 * nn)); TRY(dalloc(&c->d_lpos, nn));
-    TRY(dalloc(&c->d_evt, ne)); TRY(dalloc(&c->d_evab, ne));
-    if (!c->d_track_next) TRY(dalloc(&c->d_track_next, 1));
+// Per-track particle slots 2*len + 512 and event slots 8*len + 8192 (the
+// kernels' tbase / ebase), per-warp heap overflow hcap = 4*cap + 4096 with
+// cap = 2*maxlen + 512 the largest track's particle slots.
+static int irt_ensure(wgdna_ctx* c, uint32_t nseg, uint64_t rad_n, uint32_t cap) {
+    size_t slots = 2 * (size_t)rad_n + 512 * (size_t)nseg;
+    size_t evslots = 8 * (size_t)rad_n + 8192 * (size_t)nseg;
+    uint32_t hcap = cap * 4u + 4096u;
+    size_t hov = (size_t)irt_warps(c->device) * hcap;
+    if (slots > c->irt_slots) {
+        TRY(dalloc(&c->d_px, slots)); TRY(dalloc(&c->d_py, slots)); TRY(dalloc(&c->d_pz, slots));
+        TRY(dalloc(&c->d_tb, slots)); TRY(dalloc(&c->d_sp, slots)); TRY(dalloc(&c->d_alive8, slots));
+        TRY(dalloc(&c->d_lst, 6 * slots)); TRY(dalloc(&c->d_lpos, slots));
+        c->irt_slots = slots;
+    }
+    if (evslots > c->irt_evslots) {
+        TRY(dalloc(&c->d_evt, evslots)); TRY(dalloc(&c->d_evab, evslots));
+        c->irt_evslots = evslots;
+    }
+    if (hov > c->irt_hov) {
+        TRY(dalloc(&c->d_hov_t, hov)); TRY(dalloc(&c->d_hov_ab, hov));
+        c->irt_hov = hov;
+    }
+    c->irt_hcap = (uint32_t)(hov / irt_warps(c->device));
+    if (nseg > c->irt_tracks) {
+        TRY(dalloc(&c->d_track, 10 * (size_t)nseg)); TRY(dalloc(&c->d_toff, (size_t)nseg + 1));
+        c->irt_tracks = nseg;
+    }
+    if (!c->d_irt_cnt) TRY(dalloc(&c->d_irt_cnt, 4));
     if (!c->d_acc_tl) TRY(dalloc(&c->d_acc_tl, 35));
     if (!c->d_acc) TRY(dalloc(&c->d_acc, 16));
-    c->irt_cap = cap; c->irt_ecap = ecap; c->irt_warps = warps;
     static bool consts = false;
     if (!consts) {
         IrtConst C;
@@ -367,14 +393,13 @@ static int irt_run(wgdna_ctx* c, uint32_t nseg, uint32_t n_therm, double E_eV, u
         wg_set_error("wgdna_irt: a track of %llu entries exceeds the 32,511-entry limit of the event encoding", maxseg);
         return WGDNA_ERR_CAPACITY;
     }
-    TRY(irt_ensure(c, cap));
-    WG_CUDA_OK(cudaMemsetAsync(c->d_track_next, 0, 4, s));
+    TRY(irt_ensure(c, nseg, chem_n, cap));
     WG_CUDA_OK(cudaMemsetAsync(c->d_acc_tl, 0, 35 * 8, s));
     WG_CUDA_OK(cudaMemsetAsync(c->d_acc, 0, 16 * 8, s));
     WG_CUDA_OK(cudaMemsetAsync(c->d_err, 0, 4, s));
     IArgs a = make_iargs(c, nseg, seed);
     WG_CUDA_OK(cudaEventRecord(c->ev[4], s));
-    WG_CUDA_OK(launch_irt(a, (int)(c->irt_warps / 4), s));
+    WG_CUDA_OK(launch_irt(a, c->device, s));
     WG_CUDA_OK(cudaEventRecord(c->ev[5], s));
     double tl[35];
     unsigned long long acc[16];

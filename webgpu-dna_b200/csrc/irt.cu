@@ -226,53 +226,50 @@ __device__ void warp_sort(double* T, uint32_t* AB, uint32_t n, int lane) {
 
 constexpr uint32_t FULL = 0xffffffffu;
 
-__global__ void __launch_bounds__(IB) k_irt(IArgs A) {
-    __shared__ double s_tl[IB / 32][35];
-    __shared__ double s_ht[IB / 32][HS];
-    __shared__ uint32_t s_hab[IB / 32][HS];
-    __shared__ IrtConst s_c;
-    __shared__ uint32_t s_row[6];
-    __shared__ int s_lc[IB / 32][6];
-    for (int k = threadIdx.x; k < (int)(sizeof(IrtConst) / 4); k += IB)
-        reinterpret_cast<uint32_t*>(&s_c)[k] = reinterpret_cast<const uint32_t*>(&c_irt)[k];
+// Per-track storage (one track = one primary): particle slots at
+// tbase(p) = 2*seg_off[p] + 512*p with capacity 2*len + 512 (len = the
+// track's rad_buf entries), initial-event slots at ebase(p) =
+// 8*seg_off[p] + 8192*p: up to ecap(p) = 4*len + 4096 events, twice that
+// room for the power-of-two padding of the sort.
+__device__ __forceinline__ unsigned long long tbase(const IArgs& A, uint32_t p) { return 2ull * A.seg_off[p] + 512ull * p; }
+__device__ __forceinline__ uint32_t tcap(const IArgs& A, uint32_t p) { return (uint32_t)(2ull * (A.seg_off[p + 1] - A.seg_off[p]) + 512ull); }
+__device__ __forceinline__ unsigned long long ebase(const IArgs& A, uint32_t p) { return 8ull * A.seg_off[p] + 8192ull * p; }
+__device__ __forceinline__ uint32_t ecap(const IArgs& A, uint32_t p) { return (uint32_t)(4ull * (A.seg_off[p + 1] - A.seg_off[p]) + 4096ull); }
+
+__device__ __forceinline__ void load_consts(IrtConst* dst, uint32_t* row) {
+    for (int k = threadIdx.x; k < (int)(sizeof(IrtConst) / 4); k += blockDim.x)
+        reinterpret_cast<uint32_t*>(dst)[k] = reinterpret_cast<const uint32_t*>(&c_irt)[k];
     __syncthreads();
     if (threadIdx.x < 6) {
-        uint32_t row = 0;           // reaction index of (s, q) in 4-bit fields, 15 = none
-        for (int q = 5; q >= 0; --q) row = (row << 4) | (uint32_t)(s_c.map[threadIdx.x * 6 + q] & 15);
-        s_row[threadIdx.x] = row;
+        uint32_t r = 0;             // reaction index of (s, q) in 4-bit fields, 15 = none
+        for (int q = 5; q >= 0; --q) r = (r << 4) | (uint32_t)(dst->map[threadIdx.x * 6 + q] & 15);
+        row[threadIdx.x] = r;
     }
-    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
-    const unsigned lt = (1u << lane) - 1u;
-    const uint32_t gw = blockIdx.x * (IB / 32) + wl;
-    const IrtConst& C = s_c;
-    for (int k = lane; k < 35; k += 32) s_tl[wl][k] = 0.0;
     __syncthreads();
-    double* px = A.px + (size_t)gw * A.cap;
-    double* py = A.py + (size_t)gw * A.cap;
-    double* pz = A.pz + (size_t)gw * A.cap;
-    double* tb = A.tb + (size_t)gw * A.cap;
-    int8_t* sp = A.sp + (size_t)gw * A.cap;
-    uint8_t* alive = A.alive + (size_t)gw * A.cap;
-    uint16_t* lst = A.lst + (size_t)gw * 6 * A.cap;
-    uint16_t* lpos = A.lpos + (size_t)gw * A.cap;
-    int* lc = s_lc[wl];
-    double* ET = A.ev_t + (size_t)gw * 2 * A.ecap;          // [0, ecap): initial events
-    uint32_t* EAB = A.ev_ab + (size_t)gw * 2 * A.ecap;
-    Heap H{s_ht[wl], s_hab[wl], ET + A.ecap, EAB + A.ecap};  // product events
-    unsigned long long rxn[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    unsigned long long n_reacted = 0, n_pairs = 0, n_events = 0, n_tracks = 0;
+}
 
+// 1) load + thermalisation displacement (:475-537) and species lists; one warp per track
+__global__ void __launch_bounds__(IB) k_irt_load(IArgs A) {
+    __shared__ IrtConst s_c;
+    __shared__ uint32_t s_row[6];
+    load_consts(&s_c, s_row);
+    const IrtConst& C = s_c;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    unsigned long long n_tracks = 0;
     for (;;) {
         uint32_t p = 0;
-        if (lane == 0) p = atomicAdd(A.track_next, 1u);
+        if (lane == 0) p = atomicAdd(&A.counters[0], 1u);
         p = __shfl_sync(FULL, p, 0);
         if (p >= A.nseg) break;
         unsigned long long s = A.seg_off[p], e = A.seg_off[p + 1];
-        if (s == e) continue;
         const uint32_t pid = A.pid_base + p;
-        // ---------------------------------------------------------- load (:475-537)
+        const uint32_t cap = tcap(A, p);
+        const unsigned long long tb0 = tbase(A, p);
+        double* px = A.px + tb0; double* py = A.py + tb0; double* pz = A.pz + tb0; double* tb = A.tb + tb0;
+        int8_t* sp = A.sp + tb0; uint8_t* alive = A.alive + tb0;
+        uint16_t* lst = A.lst + 6 * tb0; uint16_t* lpos = A.lpos + tb0;
         uint32_t n = 0, h2 = 0;
-        bool overflow = false;
         for (unsigned long long c = s; c < e; c += 32) {
             unsigned long long idx = c + lane;
             bool valid = idx < e;
@@ -283,7 +280,7 @@ __global__ void __launch_bounds__(IB) k_irt(IArgs A) {
             h2 += __popc(__ballot_sync(FULL, valid && code == 7));
             unsigned m = __ballot_sync(FULL, keep);
             uint32_t k = n + __popc(m & lt);
-            if (keep && k < A.cap) {
+            if (keep) {
                 double x = r.x, y = r.y, z = r.z;
                 int spc = code;
                 double sigma = 0;
@@ -313,12 +310,8 @@ __global__ void __launch_bounds__(IB) k_irt(IArgs A) {
                 px[k] = x; py[k] = y; pz[k] = z; tb[k] = 0.0;
                 sp[k] = (int8_t)spc; alive[k] = 1;
             }
-            if (keep && k >= A.cap) overflow = true;
             n += __popc(m);
         }
-        if (__any_sync(FULL, overflow)) { if (lane == 0) atomicOr(A.err, DERR_TRACK_SIZE); continue; }
-        if (n == 0) continue;
-        n_tracks++;
         __syncwarp();
         __threadfence_block();
         uint32_t cnt[6] = {0, 0, 0, 0, 0, 0};
@@ -329,87 +322,167 @@ __global__ void __launch_bounds__(IB) k_irt(IArgs A) {
                 unsigned m = __ballot_sync(FULL, spc == q);
                 if (spc == q) {
                     uint32_t at = cnt[q] + __popc(m & lt);
-                    lst[q * A.cap + at] = (uint16_t)k;
+                    lst[q * cap + at] = (uint16_t)k;
                     lpos[k] = (uint16_t)at;
                 }
                 cnt[q] += __popc(m);
             }
         }
-        if (lane < 6) lc[lane] = (int)cnt[lane];
-        __syncwarp();
-        // -------------------------------------------------- initial pairing (:539-558)
-        uint32_t nev = 0;
+        if (lane < 6) A.tlc[6 * p + lane] = cnt[lane];
+        if (lane == 0) {
+            A.tn[p] = n;
+            A.th2[p] = h2;
+            A.ttiles[p] = (n + 31) / 32;
+            A.tev[p] = 0;
+        }
+        if (n) n_tracks++;
+    }
+    if (lane == 0 && n_tracks) atomicAdd(&A.acc[12], n_tracks);
+}
+
+// 2) initial pairing (:539-558): one warp per (track, tile of 32 particles);
+//    the 32 particles sit in lane registers, partners j are broadcast 32 at a time
+__global__ void __launch_bounds__(IB) k_irt_init(IArgs A) {
+    __shared__ IrtConst s_c;
+    __shared__ uint32_t s_row[6];
+    load_consts(&s_c, s_row);
+    const IrtConst& C = s_c;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const unsigned long long nitems = A.toff[A.nseg];
+    unsigned long long n_pairs = 0;
+    for (;;) {
+        unsigned long long item = 0;
+        if (lane == 0) item = atomicAdd(&A.counters[1], 1u);
+        item = __shfl_sync(FULL, item, 0);
+        if (item >= nitems) break;
+        uint32_t lo = 0, hi = A.nseg;                 // last p with toff[p] <= item
+        while (hi - lo > 1) { uint32_t mid = (lo + hi) >> 1; if (A.toff[mid] <= item) lo = mid; else hi = mid; }
+        const uint32_t p = lo;
+        const uint32_t pid = A.pid_base + p;
+        const uint32_t n = A.tn[p];
+        const uint32_t i0 = 32u * (uint32_t)(item - A.toff[p]);
+        const unsigned long long tb0 = tbase(A, p);
+        const double* px = A.px + tb0; const double* py = A.py + tb0; const double* pz = A.pz + tb0;
+        const int8_t* sp = A.sp + tb0;
+        double* ET = A.ev_t + ebase(A, p);
+        uint32_t* EAB = A.ev_ab + ebase(A, p);
+        const uint32_t ecp = ecap(A, p);
+        uint32_t i = i0 + lane;
+        bool hi_ = i < n;
+        double xi = 0, yi = 0, zi = 0, Di = 0;
+        int si = 0;
+        if (hi_) { xi = px[i]; yi = py[i]; zi = pz[i]; si = sp[i]; Di = C.D[si]; }
+        uint32_t row = s_row[si];
+        uint32_t cblk = 0xffffffffu;
+        u4 cw = {0, 0, 0, 0};
         bool ev_over = false;
-        for (uint32_t i0 = 0; i0 < n; i0 += 32) {
-            uint32_t i = i0 + lane;
-            bool hi = i < n;
-            double xi = 0, yi = 0, zi = 0, Di = 0;
-            int si = 0;
-            if (hi) { xi = px[i]; yi = py[i]; zi = pz[i]; si = sp[i]; Di = C.D[si]; }
-            uint32_t row = s_row[si];
-            uint32_t cblk = 0xffffffffu;
-            u4 cw = {0, 0, 0, 0};
-            for (uint32_t j0 = i0; j0 < n; j0 += 32) {
-                uint32_t jl = j0 + lane;
-                double cx = 0, cy = 0, cz = 0;
-                int cs = 0;
-                if (jl < n) { cx = px[jl]; cy = py[jl]; cz = pz[jl]; cs = sp[jl]; }
-                uint32_t kmax = min(32u, n - j0);
-                for (uint32_t kk = 0; kk < kmax; ++kk) {
-                    uint32_t j = j0 + kk;
-                    double xj = __shfl_sync(FULL, cx, kk), yj = __shfl_sync(FULL, cy, kk), zj = __shfl_sync(FULL, cz, kk);
-                    int sj = __shfl_sync(FULL, cs, kk);
-                    bool acc = false, pdcq = false;
-                    double t = 0, pa = 0, pb = 0, pD = 0;
-                    if (hi && j > i) {
-                        int ri = (int)((row >> (4 * sj)) & 15u);
-                        if (ri != 15) {
-                            double dx = xi - xj, dy = yi - yj, dz = zi - zj;
-                            double r2 = dx * dx + dy * dy + dz * dz;
-                            if (r2 <= C.r_cut2) {
-                                n_pairs++;
-                                if ((j >> 2) != cblk) { cblk = j >> 2; cw = philox(cblk, i, pid, 3u, A.k0, A.k1); }
-                                uint32_t wd = (j & 3) == 0 ? cw.x : (j & 3) == 1 ? cw.y : (j & 3) == 2 ? cw.z : cw.w;
-                                double U = u01d32(wd);
-                                double R = r_acc(C, ri, U);
-                                if (r2 <= R * R) {
-                                    double D = Di + C.D[sj];
-                                    t = sample_pre(C, sqrt(r2), ri, D, U, &pa, &pb);
-                                    if (t == -2.0) { pdcq = true; pD = D; }
-                                    else acc = (t >= 0 && t < 1000);
-                                }
+        for (uint32_t j0 = i0; j0 < n; j0 += 32) {
+            uint32_t jl = j0 + lane;
+            double cx = 0, cy = 0, cz = 0;
+            int cs = 0;
+            if (jl < n) { cx = px[jl]; cy = py[jl]; cz = pz[jl]; cs = sp[jl]; }
+            uint32_t kmax = min(32u, n - j0);
+            for (uint32_t kk = 0; kk < kmax; ++kk) {
+                uint32_t j = j0 + kk;
+                double xj = __shfl_sync(FULL, cx, kk), yj = __shfl_sync(FULL, cy, kk), zj = __shfl_sync(FULL, cz, kk);
+                int sj = __shfl_sync(FULL, cs, kk);
+                bool acc = false, pdcq = false;
+                double t = 0, pa = 0, pb = 0, pD = 0;
+                if (hi_ && j > i) {
+                    int ri = (int)((row >> (4 * sj)) & 15u);
+                    if (ri != 15) {
+                        double dx = xi - xj, dy = yi - yj, dz = zi - zj;
+                        double r2 = dx * dx + dy * dy + dz * dz;
+                        if (r2 <= C.r_cut2) {
+                            n_pairs++;
+                            if ((j >> 2) != cblk) { cblk = j >> 2; cw = philox(cblk, i, pid, 3u, A.k0, A.k1); }
+                            uint32_t wd = (j & 3) == 0 ? cw.x : (j & 3) == 1 ? cw.y : (j & 3) == 2 ? cw.z : cw.w;
+                            double U = u01d32(wd);
+                            double R = r_acc(C, ri, U);
+                            if (r2 <= R * R) {
+                                double D = Di + C.D[sj];
+                                t = sample_pre(C, sqrt(r2), ri, D, U, &pa, &pb);
+                                if (t == -2.0) { pdcq = true; pD = D; }
+                                else acc = (t >= 0 && t < 1000);
                             }
                         }
                     }
-                    unsigned pm = __ballot_sync(FULL, pdcq);
-                    while (pm) {
-                        int src = __ffs(pm) - 1;
-                        pm &= pm - 1;
-                        uint32_t qi = __shfl_sync(FULL, i, src);
-                        double qa = __shfl_sync(FULL, pa, src), qb = __shfl_sync(FULL, pb, src);
-                        double X = pdc_warp(qi, j, pid, A.k0, A.k1, qa, qb, lane);
-                        if (lane == src && X > 0) { t = X / pD; acc = t < 1000; }
-                    }
-                    unsigned m = __ballot_sync(FULL, acc);
-                    if (m) {
-                        uint32_t slot = nev + __popc(m & lt);
-                        if (acc) {
-                            if (slot < A.ecap) { ET[slot] = t; EAB[slot] = (i << 16) | j; }
-                            else ev_over = true;
-                        }
-                        nev += __popc(m);
+                }
+                unsigned pm = __ballot_sync(FULL, pdcq);
+                while (pm) {
+                    int src = __ffs(pm) - 1;
+                    pm &= pm - 1;
+                    uint32_t qi = __shfl_sync(FULL, i, src);
+                    double qa = __shfl_sync(FULL, pa, src), qb = __shfl_sync(FULL, pb, src);
+                    double X = pdc_warp(qi, j, pid, A.k0, A.k1, qa, qb, lane);
+                    if (lane == src && X > 0) { t = X / pD; acc = t < 1000; }
+                }
+                unsigned m = __ballot_sync(FULL, acc);
+                if (m) {
+                    uint32_t base = 0;
+                    if (lane == 0) base = atomicAdd(&A.tev[p], (uint32_t)__popc(m));
+                    base = __shfl_sync(FULL, base, 0);
+                    uint32_t slot = base + __popc(m & lt);
+                    if (acc) {
+                        if (slot < ecp) { ET[slot] = t; EAB[slot] = (i << 16) | j; }
+                        else ev_over = true;
                     }
                 }
             }
         }
-        if (__any_sync(FULL, ev_over)) { if (lane == 0) atomicOr(A.err, DERR_HEAP); continue; }
+        if (__any_sync(FULL, ev_over) && lane == 0) atomicOr(A.err, DERR_HEAP);
+    }
+    for (int o = 16; o; o >>= 1) n_pairs += __shfl_xor_sync(FULL, n_pairs, o);
+    if (lane == 0 && n_pairs) atomicAdd(&A.acc[10], n_pairs);
+}
+
+// 3) events (:566-660): sort the initial events, then pop in (t, i, j) order
+//    merged with a heap of product events; one warp per track
+__global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
+    __shared__ double s_tl[IB / 32][35];
+    __shared__ double s_ht[IB / 32][HS];
+    __shared__ uint32_t s_hab[IB / 32][HS];
+    __shared__ int s_lc[IB / 32][6];
+    __shared__ IrtConst s_c;
+    __shared__ uint32_t s_row[6];
+    load_consts(&s_c, s_row);
+    const IrtConst& C = s_c;
+    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+    const uint32_t gw = blockIdx.x * (IB / 32) + wl;
+    for (int k = lane; k < 35; k += 32) s_tl[wl][k] = 0.0;
+    int* lc = s_lc[wl];
+    Heap H{s_ht[wl], s_hab[wl], A.hov_t + (size_t)gw * A.hcap, A.hov_ab + (size_t)gw * A.hcap};
+    unsigned long long rxn[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    unsigned long long n_reacted = 0, n_pairs = 0, n_events = 0;
+    __syncwarp();
+    for (;;) {
+        uint32_t p = 0;
+        if (lane == 0) p = atomicAdd(&A.counters[2], 1u);
+        p = __shfl_sync(FULL, p, 0);
+        if (p >= A.nseg) break;
+        const uint32_t n = A.tn[p];
+        if (n == 0) continue;
+        const uint32_t pid = A.pid_base + p;
+        const uint32_t cap = tcap(A, p);
+        const unsigned long long tb0 = tbase(A, p);
+        double* px = A.px + tb0; double* py = A.py + tb0; double* pz = A.pz + tb0; double* tb = A.tb + tb0;
+        int8_t* sp = A.sp + tb0; uint8_t* alive = A.alive + tb0;
+        uint16_t* lst = A.lst + 6 * tb0; uint16_t* lpos = A.lpos + tb0;
+        double* ET = A.ev_t + ebase(A, p);
+        uint32_t* EAB = A.ev_ab + ebase(A, p);
+        const uint32_t nev = A.tev[p];
+        uint32_t cnt[6];
+        for (int q = 0; q < 6; ++q) cnt[q] = A.tlc[6 * p + q];
+        if (lane < 6) lc[lane] = (int)cnt[lane];
+        uint32_t n2 = 1;
+        while (n2 < nev) n2 <<= 1;
+        if (nev > ecap(A, p)) { if (lane == 0) atomicOr(A.err, DERR_HEAP); continue; }
         __syncwarp();
-        __threadfence_block();
         warp_sort(ET, EAB, nev, lane);
-        // ------------------------------------------------------- event loop (:566-660)
         uint32_t ip = 0, hn = 0;
         uint32_t ntot = n;
-        double h2c = (double)h2;
+        double h2c = (double)A.th2[p];
         int cp = 0;
         bool heap_over = false;
         const double CP[7] = {0.001, 0.01, 0.1, 1, 10, 100, 1000};
@@ -450,8 +523,8 @@ __global__ void __launch_bounds__(IB) k_irt(IArgs A) {
                         for (int w2 = 0; w2 < 2; ++w2) {
                             int k = w2 == 0 ? ei : ej, q = w2 == 0 ? si : sj;
                             uint32_t at = lpos[k];
-                            uint16_t last = lst[q * A.cap + lc[q] - 1];
-                            lst[q * A.cap + at] = last;
+                            uint16_t last = lst[q * cap + lc[q] - 1];
+                            lst[q * cap + at] = last;
                             lpos[last] = (uint16_t)at;
                             lc[q]--;
                         }
@@ -478,7 +551,7 @@ __global__ void __launch_bounds__(IB) k_irt(IArgs A) {
             for (int pp = 0; pp < np_; ++pp) {
                 int nsp = pp == 0 ? C.prod0[ri] : C.prod1[ri];
                 uint32_t id = ntot;
-                if (id >= A.cap) break;
+                if (id >= cap) break;
                 double nx, ny, nz;
                 if (np_ == 1) { nx = mx; ny = my; nz = mz; }
                 else if (pp == 0) { nx = xa; ny = ya; nz = za; }
@@ -487,88 +560,87 @@ __global__ void __launch_bounds__(IB) k_irt(IArgs A) {
                     px[id] = nx; py[id] = ny; pz[id] = nz; tb[id] = et;
                     sp[id] = (int8_t)nsp; alive[id] = 1;
                     cnt[nsp]++;
-                    lst[nsp * A.cap + lc[nsp]] = (uint16_t)id;
+                    lst[nsp * cap + lc[nsp]] = (uint16_t)id;
                     lpos[id] = (uint16_t)lc[nsp];
                     lc[nsp]++;
                 }
                 ntot++;
                 __syncwarp();
                 __threadfence_block();
-                // pairWithAlive (:430-465)
+                // pairWithAlive (:430-465) over the alive particles of the species that react with nsp
                 double Di = C.D[nsp];
                 uint32_t rowp = s_row[nsp];
-                // partners: the alive particles of the species that react with nsp
                 for (int s2 = 0; s2 < 6; ++s2) {
-                const int r2i = (int)((rowp >> (4 * s2)) & 15u);
-                if (r2i == 15) continue;
-                const uint32_t len = (uint32_t)lc[s2];
-                for (uint32_t c0 = 0; c0 < len; c0 += 32) {
-                    uint32_t li = c0 + lane;
-                    uint32_t jj = li < len ? lst[s2 * A.cap + li] : 0u;
-                    bool cand = li < len && jj != id;
-                    bool acc = false, pdcq = false;
-                    double ta = 0, pa = 0, pb = 0, pD = 0;
-                    if (cand) {
-                        n_pairs++;
-                        double Dj = C.D[s2];
-                        double dt = et - tb[jj];
-                        double xj = px[jj], yj = py[jj], zj = pz[jj];
-                        u4 q0 = philox(id, jj, pid, 5u, A.k0, A.k1);
-                        double U = u01d32(q0.w);
-                        double R = r_acc(C, r2i, U);
-                        bool need = true;
-                        if (dt > 0) {
-                            double sig = sqrt(2.0 * Dj * dt);
-                            // |gaussian 3-vector| <= sqrt(sum -2 ln u1_k) (Box-Muller radius), with margin
-                            float l0 = -2.0f * __logf((float)u01d32(q0.x));
-                            float l1 = -2.0f * __logf((float)u01d32(q0.y));
-                            float l2 = -2.0f * __logf((float)u01d32(q0.z));
-                            double B = (double)sqrtf((l0 + l1 + l2) * 1.0001f) + 1e-4;
-                            double ex = nx - xj, ey = ny - yj, ez = nz - zj;
-                            double dist = sqrt(ex * ex + ey * ey + ez * ez);
-                            if (dist - sig * B > R) need = false;
+                    const int r2i = (int)((rowp >> (4 * s2)) & 15u);
+                    if (r2i == 15) continue;
+                    const uint32_t len = (uint32_t)lc[s2];
+                    for (uint32_t c0 = 0; c0 < len; c0 += 32) {
+                        uint32_t li = c0 + lane;
+                        uint32_t jj = li < len ? lst[s2 * cap + li] : 0u;
+                        bool cand = li < len && jj != id;
+                        bool acc = false, pdcq = false;
+                        double ta = 0, pa = 0, pb = 0, pD = 0;
+                        if (cand) {
+                            n_pairs++;
+                            double Dj = C.D[s2];
+                            double dt = et - tb[jj];
+                            double xj = px[jj], yj = py[jj], zj = pz[jj];
+                            u4 q0 = philox(id, jj, pid, 5u, A.k0, A.k1);
+                            double U = u01d32(q0.w);
+                            double R = r_acc(C, r2i, U);
+                            bool need = true;
+                            if (dt > 0) {
+                                double sig = sqrt(2.0 * Dj * dt);
+                                // |gaussian 3-vector| <= sqrt(sum -2 ln u1_k) (Box-Muller radius), with margin
+                                float l0 = -2.0f * __logf((float)u01d32(q0.x));
+                                float l1 = -2.0f * __logf((float)u01d32(q0.y));
+                                float l2 = -2.0f * __logf((float)u01d32(q0.z));
+                                double B = (double)sqrtf((l0 + l1 + l2) * 1.0001f) + 1e-4;
+                                double ex = nx - xj, ey = ny - yj, ez = nz - zj;
+                                double dist = sqrt(ex * ex + ey * ey + ez * ez);
+                                if (dist - sig * B > R) need = false;
+                                if (need) {
+                                    u4 q1 = philox(id, jj, pid, 5u | (1u << 4), A.k0, A.k1);
+                                    double g0 = sqrt(-2 * log_(u01d32(q0.x) + 1e-30)) * cos_(6.2831853 * u01d32(q1.x));
+                                    double g1 = sqrt(-2 * log_(u01d32(q0.y) + 1e-30)) * cos_(6.2831853 * u01d32(q1.y));
+                                    double g2 = sqrt(-2 * log_(u01d32(q0.z) + 1e-30)) * cos_(6.2831853 * u01d32(q1.z));
+                                    xj += g0 * sig; yj += g1 * sig; zj += g2 * sig;
+                                }
+                            }
                             if (need) {
-                                u4 q1 = philox(id, jj, pid, 5u | (1u << 4), A.k0, A.k1);
-                                double g0 = sqrt(-2 * log_(u01d32(q0.x) + 1e-30)) * cos_(6.2831853 * u01d32(q1.x));
-                                double g1 = sqrt(-2 * log_(u01d32(q0.y) + 1e-30)) * cos_(6.2831853 * u01d32(q1.y));
-                                double g2 = sqrt(-2 * log_(u01d32(q0.z) + 1e-30)) * cos_(6.2831853 * u01d32(q1.z));
-                                xj += g0 * sig; yj += g1 * sig; zj += g2 * sig;
+                                double dx = nx - xj, dy = ny - yj, dz = nz - zj;
+                                double r2 = dx * dx + dy * dy + dz * dz;
+                                if (r2 <= C.r_cut2) {
+                                    double D = Di + Dj;
+                                    double t = sample_pre(C, sqrt(r2), r2i, D, U, &pa, &pb);
+                                    if (t == -2.0) { pdcq = true; pD = D; }
+                                    else if (t >= 0) { ta = et + t; acc = ta < 1000; }
+                                }
                             }
                         }
-                        if (need) {
-                            double dx = nx - xj, dy = ny - yj, dz = nz - zj;
-                            double r2 = dx * dx + dy * dy + dz * dz;
-                            if (r2 <= C.r_cut2) {
-                                double D = Di + Dj;
-                                double t = sample_pre(C, sqrt(r2), r2i, D, U, &pa, &pb);
-                                if (t == -2.0) { pdcq = true; pD = D; }
-                                else if (t >= 0) { ta = et + t; acc = ta < 1000; }
+                        unsigned pm = __ballot_sync(FULL, pdcq);
+                        while (pm) {
+                            int src = __ffs(pm) - 1;
+                            pm &= pm - 1;
+                            uint32_t qj = __shfl_sync(FULL, jj, src);
+                            double qa = __shfl_sync(FULL, pa, src), qb = __shfl_sync(FULL, pb, src);
+                            double X = pdc_warp(id, qj, pid, A.k0, A.k1, qa, qb, lane);
+                            if (lane == src && X > 0) { ta = et + X / pD; acc = ta < 1000; }
+                        }
+                        unsigned m = __ballot_sync(FULL, acc);
+                        while (m) {
+                            int src = __ffs(m) - 1;
+                            m &= m - 1;
+                            double tt = __shfl_sync(FULL, ta, src);
+                            uint32_t pj = __shfl_sync(FULL, jj, src);
+                            if (lane == 0) {
+                                if (hn < HS + A.hcap) {
+                                    uint32_t a = pj < id ? pj : id, bq = pj < id ? id : pj;
+                                    heap_push(H, hn, tt, (a << 16) | bq);
+                                } else heap_over = true;
                             }
                         }
                     }
-                    unsigned pm = __ballot_sync(FULL, pdcq);
-                    while (pm) {
-                        int src = __ffs(pm) - 1;
-                        pm &= pm - 1;
-                        uint32_t qj = __shfl_sync(FULL, jj, src);
-                        double qa = __shfl_sync(FULL, pa, src), qb = __shfl_sync(FULL, pb, src);
-                        double X = pdc_warp(id, qj, pid, A.k0, A.k1, qa, qb, lane);
-                        if (lane == src && X > 0) { ta = et + X / pD; acc = ta < 1000; }
-                    }
-                    unsigned m = __ballot_sync(FULL, acc);
-                    while (m) {
-                        int src = __ffs(m) - 1;
-                        m &= m - 1;
-                        double tt = __shfl_sync(FULL, ta, src);
-                        uint32_t pj = __shfl_sync(FULL, jj, src);
-                        if (lane == 0) {
-                            if (hn < HS + A.ecap) {
-                                uint32_t a = pj < id ? pj : id, bq = pj < id ? id : pj;
-                                heap_push(H, hn, tt, (a << 16) | bq);
-                            } else heap_over = true;
-                        }
-                    }
-                }
                 }
                 __syncwarp();
                 __threadfence_block();
@@ -590,8 +662,8 @@ __global__ void __launch_bounds__(IB) k_irt(IArgs A) {
         for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
         if (lane == 0 && v) atomicAdd(&A.acc[k], v);
     }
-    unsigned long long vals[4] = {n_reacted, n_pairs, n_events, n_tracks};
-    for (int k = 0; k < 4; ++k) {
+    unsigned long long vals[3] = {n_reacted, n_pairs, n_events};
+    for (int k = 0; k < 3; ++k) {
         unsigned long long v = vals[k];
         for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
         if (lane == 0 && v) atomicAdd(&A.acc[9 + k], v);
@@ -627,16 +699,26 @@ __global__ void k_seg_max(const unsigned long long* off, uint32_t nseg, unsigned
 // ------------------------------------------------------------------ host side
 cudaError_t irt_set_constants(const IrtConst& c) { return cudaMemcpyToSymbol(c_irt, &c, sizeof c); }
 
-int irt_blocks(int device) {
+static int blocks_for(const void* k, int device) {
     int sms = 0, per = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_irt, IB, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, IB, 0);
     if (per < 1) per = 1;
     return sms * per;
 }
 
-cudaError_t launch_irt(const IArgs& a, int blocks, cudaStream_t s) {
-    k_irt<<<blocks, IB, 0, s>>>(a);
+int irt_warps(int device) { return blocks_for((const void*)k_irt_loop, device) * (IB / 32); }
+
+// tile prefix: the scan of transport.cu
+cudaError_t launch_scan_u32(const uint32_t* cnt, uint32_t n, unsigned long long* off, cudaStream_t s);
+
+cudaError_t launch_irt(const IArgs& a, int device, cudaStream_t s) {
+    cudaMemsetAsync(a.counters, 0, 4 * sizeof(uint32_t), s);
+    k_irt_load<<<blocks_for((const void*)k_irt_load, device), IB, 0, s>>>(a);
+    cudaError_t e = launch_scan_u32(a.ttiles, a.nseg, a.toff, s);
+    if (e != cudaSuccess) return e;
+    k_irt_init<<<blocks_for((const void*)k_irt_init, device), IB, 0, s>>>(a);
+    k_irt_loop<<<blocks_for((const void*)k_irt_loop, device), IB, 0, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -17,24 +17,30 @@ struct IrtConst {
 struct IArgs {
     const float4* rad;
     const unsigned long long* seg_off;   // nseg + 1
-    uint32_t nseg, k0, k1, cap, ecap, nwarps;
-    uint32_t pid_base;                   // global id of segment 0
-    double *px, *py, *pz, *tb;           // [warp][cap]
+    uint32_t nseg, k0, k1, pid_base;
+    // per-track storage (irt.cu tbase / ebase)
+    double *px, *py, *pz, *tb;
     int8_t* sp;
     uint8_t* alive;
-    uint16_t* lst;                       // [warp][6][cap]: alive particles of each species
-    uint16_t* lpos;                      // [warp][cap]: position of a particle in its list
-    double* ev_t;                        // [warp][2*ecap]: initial events, then heap overflow
+    uint16_t* lst;                       // 6 lists per track: alive particles of each species
+    uint16_t* lpos;                      // position of a particle in its list
+    double* ev_t;                        // initial events of each track
     uint32_t* ev_ab;                     // packed (a << 16) | b
-    uint32_t* track_next;
+    uint32_t *tn, *th2, *ttiles, *tev, *tlc;   // per track: particles, H2 markers, tiles, events, 6 list lengths
+    unsigned long long* toff;            // nseg + 1: prefix of ttiles
+    // per-warp heap overflow of the event kernel
+    double* hov_t;
+    uint32_t* hov_ab;
+    uint32_t hcap;
+    uint32_t* counters;                  // [0] load, [1] init items, [2] loop tracks
     double* acc_tl;                      // 35
     unsigned long long* acc;             // [0..8] rxn, 9 reacted, 10 pairs, 11 events, 12 tracks
     uint32_t* err;
 };
 
 cudaError_t irt_set_constants(const IrtConst& c);
-int irt_blocks(int device);
-cudaError_t launch_irt(const IArgs& a, int blocks, cudaStream_t s);
+int irt_warps(int device);
+cudaError_t launch_irt(const IArgs& a, int device, cudaStream_t s);
 cudaError_t launch_group_keys(const float4* rad, unsigned long long n, unsigned long long* key, uint32_t* maxpid,
                               cudaStream_t s);
 cudaError_t launch_seg_max(const unsigned long long* off, uint32_t nseg, unsigned long long* out, cudaStream_t s);

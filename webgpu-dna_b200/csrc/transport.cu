@@ -940,6 +940,11 @@ cudaError_t launch_canon(const unsigned long long* key, const float4* rad, unsig
     return cudaGetLastError();
 }
 
+cudaError_t launch_scan_u32(const uint32_t* cnt, uint32_t n, unsigned long long* off, cudaStream_t s) {
+    k_scan<<<1, 1024, 0, s>>>(cnt, n, off);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_reduce(const float* results, uint32_t np, const uint32_t* dose, uint32_t nvox,
                           unsigned long long* out, cudaStream_t s) {
     cudaMemsetAsync(out, 0, 16, s);
