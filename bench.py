@@ -42,6 +42,10 @@ E_EV = 10000.0
 WORKLOAD = ("4096 x 10 keV e- in liquid water, box +-15 um, cutoff 7.5 eV, Philox seed 0 -> "
             "IRT to 1 us -> direct SSB + DSB on 21x21 B-DNA fibres")
 CPU_SAMPLE_PRIMARIES = 512
+# library kernels per step: transport 1, rad_buf canonical order 5 (histogram,
+# scan, scatter, segment sort, reduce), IRT 5 (segment max, load, scan,
+# pairing, events), scoring 5 (prep, tiles, tile scan, apply, cluster)
+LAUNCHES_PER_STEP = 16
 
 
 def peaks():
@@ -227,7 +231,7 @@ def run_native(args, ws, rank, local):
         torch.cuda.synchronize()
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    t_tr, t_irt, t_canon, t_sc = [], [], [], []
+    t_tr, t_irt, t_canon, t_sc, t_pair, t_evl = [], [], [], [], [], []
     launches = 0
     with Clocks(local) as clk:
         barrier()
@@ -241,8 +245,10 @@ def run_native(args, ws, rank, local):
             t_tr.append(st.ms_transport)
             t_canon.append(st.ms_canon)
             t_irt.append(ir.ms)
+            t_pair.append(ir.ms_pairing)
+            t_evl.append(ir.ms_events)
             t_sc.append(ssb.ms + dsb.ms)
-            launches += 13
+            launches += LAUNCHES_PER_STEP
         barrier()
     ms = [a.elapsed_time(b) for a, b in ev]
     tot_ms = sum(ms)
@@ -271,20 +277,28 @@ def run_native(args, ws, rank, local):
     pk = peaks()
     mean = lambda a: sum(a) / len(a)
     stages = {"irt": mean(t_irt), "transport": mean(t_tr), "canon": mean(t_canon), "scoring": mean(t_sc)}
-    dom = max(stages, key=stages.get)
-    R, S = st.rad_n_stored, st.sec_n
-    if dom == "transport":
-        alg = 16 * R + 8 * R + 96 * S + 32 * NPr
-    elif dom == "irt":
-        alg = 16 * R + 34 * R + 16 * ir.n_events
-    else:
-        alg = 16 * R
-    achieved = alg / (stages[dom] / 1000.0) / 1e9
+    kernels = {"k_transport": mean(t_tr), "k_irt_init": mean(t_pair), "k_irt_loop": mean(t_evl)}
+    dom = max(kernels, key=kernels.get)
+    R, S, D = st.rad_n_stored, st.sec_n, st.dbg[5]
+    Np, Ei, Et = ir.n_particles, ir.n_init_events, ir.n_events
+    alg = {
+        # rad_buf 16 B/entry, secondaries pushed + popped 48 B each, R struct 32 B, dose atomics 4 B
+        "k_transport": 16 * R + 96 * S + 32 * NPr + 4 * D,
+        # tracked species (x, y, z f64 + species) read once, initial events (t f64, ids u32) written once
+        "k_irt_init": 25 * Np + 12 * Ei,
+        # initial events read once, species state read, product events pushed and popped
+        "k_irt_loop": 12 * Ei + 25 * Np + 24 * max(Et - Ei, 0),
+    }[dom]
+    achieved = alg / (kernels[dom] / 1000.0) / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
         try:
-            traffic = json.load(open(tf)).get(dom)
+            t = json.load(open(tf)).get(dom)
+            # dram bytes per full launch, scaled from the profiled case by the units processed
+            if t:
+                unit = {"k_transport": NPr, "k_irt_init": Np, "k_irt_loop": Np}[dom]
+                traffic = t["bytes_per_unit"] * unit
         except Exception:
             traffic = None
     clocks = clk.summary()
@@ -301,12 +315,15 @@ def run_native(args, ws, rank, local):
                     "d2h_bytes_per_step": e2e_bytes["d2h"]},
             "gpu_launches": launches,
             "stage_ms": {k: round(v, 4) for k, v in stages.items()},
+            "kernel_ms": {k: round(v, 4) for k, v in kernels.items()},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk["hbm_gbs"],
                          "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
+                         "alg_bytes": int(alg),
                          "peak_source": "fallback" if pk.get("fallback") else "measured"},
             "clocks": clocks,
             "work": {"rad_n": int(R), "sec_n": int(S), "steps": int(st.steps), "irt_pairs": int(ir.n_pairs),
-                     "irt_events": int(ir.n_events), "ssb": int(ssb.ssb), "dsb": int(dsb.dsb)},
+                     "irt_events": int(ir.n_events), "irt_init_events": int(Ei), "irt_species": int(Np),
+                     "dose_atomics": int(D), "ssb": int(ssb.ssb), "dsb": int(dsb.dsb)},
         }
         if ws == 1 and not args.no_cpu:
             nthreads = os.cpu_count() or 1

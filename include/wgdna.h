@@ -72,7 +72,7 @@ typedef struct {
 typedef struct {
     uint32_t counters[8];       /* primary.wgsl:24-35: OH, eaq, H, H3O+, DNA hits, H2, sec idx, rad idx */
     uint32_t sec_stats[8];      /* [1] cutoff, [2] bounds, [3] steps, [4] tertiary ions */
-    uint32_t dbg[8];            /* [0] ions, [1] exc, [2] escaped, [3] primaries, [4] sum W*10 */
+    uint32_t dbg[8];            /* [0] ions, [1] exc, [2] escaped, [3] primaries, [4] sum W*10, [5] dose-grid atomics */
     uint64_t rad_n_raw, rad_n_stored, rad_dropped;
     uint64_t sec_n_raw, sec_n, sec_dropped;
     uint64_t dep_units;         /* sum of the dose grid (100 units per eV) */
@@ -104,8 +104,10 @@ typedef struct {
     double G[7][5];             /* per 100 eV of n_therm * E_eV (irt-worker.js:670-682) */
     uint64_t rxn_counts[9];     /* irt-worker.js:685-694 order */
     uint64_t n_reacted, n_tracks, n_pairs, n_events;
+    uint64_t n_particles, n_init_events;   /* tracked species loaded; events from the initial pairing */
     uint64_t chem_n;
-    float ms;
+    float ms;                   /* whole IRT on the device */
+    float ms_load, ms_pairing, ms_events;   /* its kernels: load + displacement, initial pairing, event loop */
     uint32_t device_error;
 } wgdna_irt_result;
 

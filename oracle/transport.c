@@ -258,6 +258,7 @@ static void deposit(emit_t *e, float px, float py, float pz, float dep) {  /* pr
     uint32_t u = (uint32_t)(dep * 100.0f);
     if (e->sk->dose) e->sk->dose[(uint32_t)((iz * n + iy) * n + ix)] += u;
     e->sk->dep_units += u;
+    e->sk->dbg[5] += 1u;                 /* dose-grid updates (an instrumentation count) */
 }
 
 static uint32_t dna_near(const orc_transport_params *p, float px, float py, float pz) {

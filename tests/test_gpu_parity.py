@@ -37,7 +37,7 @@ def assert_transport_equal(st, res, dose, rad, o):
     np.testing.assert_array_equal(res.view(np.uint32), o["results"].view(np.uint32))
     np.testing.assert_array_equal(np.array(st.counters[:]), o["counters"])
     np.testing.assert_array_equal(np.array(st.sec_stats[:]), o["sec_stats"])
-    np.testing.assert_array_equal(np.array(st.dbg[:5]), o["dbg"][:5])
+    np.testing.assert_array_equal(np.array(st.dbg[:6]), o["dbg"][:6])
     assert st.rad_dropped == 0 and st.sec_dropped == 0
     assert rad.shape == o["rad"].shape
     np.testing.assert_array_equal(rad.view(np.uint32), o["rad"].view(np.uint32))

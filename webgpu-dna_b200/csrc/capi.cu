@@ -82,7 +82,7 @@ struct wgdna_ctx {
     double* d_acc_tl = nullptr;
     unsigned long long* d_acc = nullptr;
     uint32_t* d_maxpid = nullptr;
-    cudaEvent_t ev[8]{};
+    cudaEvent_t ev[10]{};
 };
 
 static std::string lib_dir() {
@@ -399,7 +399,7 @@ static int irt_run(wgdna_ctx* c, uint32_t nseg, uint32_t n_therm, double E_eV, u
     WG_CUDA_OK(cudaMemsetAsync(c->d_err, 0, 4, s));
     IArgs a = make_iargs(c, nseg, seed);
     WG_CUDA_OK(cudaEventRecord(c->ev[4], s));
-    WG_CUDA_OK(launch_irt(a, c->device, s));
+    WG_CUDA_OK(launch_irt(a, c->device, s, &c->ev[8]));
     WG_CUDA_OK(cudaEventRecord(c->ev[5], s));
     double tl[35];
     unsigned long long acc[16];
@@ -418,8 +418,12 @@ static int irt_run(wgdna_ctx* c, uint32_t nseg, uint32_t n_therm, double E_eV, u
             }
         for (int r = 0; r < 9; ++r) out->rxn_counts[r] = acc[r];
         out->n_reacted = acc[9]; out->n_pairs = acc[10]; out->n_events = acc[11]; out->n_tracks = acc[12];
+        out->n_particles = acc[13]; out->n_init_events = acc[14];
         out->chem_n = chem_n;
         cudaEventElapsedTime(&out->ms, c->ev[4], c->ev[5]);
+        cudaEventElapsedTime(&out->ms_load, c->ev[4], c->ev[8]);
+        cudaEventElapsedTime(&out->ms_pairing, c->ev[8], c->ev[9]);
+        cudaEventElapsedTime(&out->ms_events, c->ev[9], c->ev[5]);
         out->device_error = err;
     }
     if (err) { wg_set_error("wgdna_irt: device error flags 0x%x", err); return WGDNA_ERR_DEVICE; }

@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(IB) k_irt_load(IArgs A) {
     const IrtConst& C = s_c;
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
-    unsigned long long n_tracks = 0;
+    unsigned long long n_tracks = 0, n_part = 0;
     for (;;) {
         uint32_t p = 0;
         if (lane == 0) p = atomicAdd(&A.counters[0], 1u);
@@ -335,9 +335,9 @@ __global__ void __launch_bounds__(IB) k_irt_load(IArgs A) {
             A.ttiles[p] = (n + 31) / 32;
             A.tev[p] = 0;
         }
-        if (n) n_tracks++;
+        if (n) { n_tracks++; n_part += n; }
     }
-    if (lane == 0 && n_tracks) atomicAdd(&A.acc[12], n_tracks);
+    if (lane == 0 && n_tracks) { atomicAdd(&A.acc[12], n_tracks); atomicAdd(&A.acc[13], n_part); }
 }
 
 // 2) initial pairing (:539-558): one warp per (track, tile of 32 particles);
@@ -454,7 +454,7 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
     int* lc = s_lc[wl];
     Heap H{s_ht[wl], s_hab[wl], A.hov_t + (size_t)gw * A.hcap, A.hov_ab + (size_t)gw * A.hcap};
     unsigned long long rxn[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    unsigned long long n_reacted = 0, n_pairs = 0, n_events = 0;
+    unsigned long long n_reacted = 0, n_pairs = 0, n_events = 0, n_init = 0;
     __syncwarp();
     for (;;) {
         uint32_t p = 0;
@@ -478,6 +478,7 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
         uint32_t n2 = 1;
         while (n2 < nev) n2 <<= 1;
         if (nev > ecap(A, p)) { if (lane == 0) atomicOr(A.err, DERR_HEAP); continue; }
+        n_init += nev;
         __syncwarp();
         warp_sort(ET, EAB, nev, lane);
         uint32_t ip = 0, hn = 0;
@@ -662,6 +663,7 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
         for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
         if (lane == 0 && v) atomicAdd(&A.acc[k], v);
     }
+    if (lane == 0 && n_init) atomicAdd(&A.acc[14], n_init);
     unsigned long long vals[3] = {n_reacted, n_pairs, n_events};
     for (int k = 0; k < 3; ++k) {
         unsigned long long v = vals[k];
@@ -712,12 +714,14 @@ int irt_warps(int device) { return blocks_for((const void*)k_irt_loop, device) *
 // tile prefix: the scan of transport.cu
 cudaError_t launch_scan_u32(const uint32_t* cnt, uint32_t n, unsigned long long* off, cudaStream_t s);
 
-cudaError_t launch_irt(const IArgs& a, int device, cudaStream_t s) {
+cudaError_t launch_irt(const IArgs& a, int device, cudaStream_t s, cudaEvent_t* ev) {
     cudaMemsetAsync(a.counters, 0, 4 * sizeof(uint32_t), s);
     k_irt_load<<<blocks_for((const void*)k_irt_load, device), IB, 0, s>>>(a);
     cudaError_t e = launch_scan_u32(a.ttiles, a.nseg, a.toff, s);
     if (e != cudaSuccess) return e;
+    if (ev) cudaEventRecord(ev[0], s);
     k_irt_init<<<blocks_for((const void*)k_irt_init, device), IB, 0, s>>>(a);
+    if (ev) cudaEventRecord(ev[1], s);
     k_irt_loop<<<blocks_for((const void*)k_irt_loop, device), IB, 0, s>>>(a);
     return cudaGetLastError();
 }

@@ -40,7 +40,8 @@ struct IArgs {
 
 cudaError_t irt_set_constants(const IrtConst& c);
 int irt_warps(int device);
-cudaError_t launch_irt(const IArgs& a, int device, cudaStream_t s);
+// ev (optional, 2 events): recorded after the load and after the initial pairing
+cudaError_t launch_irt(const IArgs& a, int device, cudaStream_t s, cudaEvent_t* ev = nullptr);
 cudaError_t launch_group_keys(const float4* rad, unsigned long long n, unsigned long long* key, uint32_t* maxpid,
                               cudaStream_t s);
 cudaError_t launch_seg_max(const unsigned long long* off, uint32_t nseg, unsigned long long* out, cudaStream_t s);

@@ -56,7 +56,7 @@ constexpr float PI_F = 3.14159265f;
 // counters inside the block's shared block: [0..7] counters, [8..15] sec_stats, [16..23] dbg
 enum { C_OH = 0, C_EAQ = 1, C_H = 2, C_H3O = 3, C_DNA = 4, C_H2 = 5,
        SS_CUT = 9, SS_BOUNDS = 10, SS_STEPS = 11, SS_TERT = 12,
-       D_IONS = 16, D_EXC = 17, D_ESC = 18, D_PRIM = 19, D_WSUM = 20, C_SECN = 22 };
+       D_IONS = 16, D_EXC = 17, D_ESC = 18, D_PRIM = 19, D_WSUM = 20, D_DOSE = 21, C_SECN = 22 };
 
 struct Particle {
     float px, py, pz, E, dx, dy, dz;
@@ -98,9 +98,12 @@ __device__ __forceinline__ void put(const TArgs& A, Blk& b, Particle& q, float x
     q.seq++;
 }
 
-__device__ __forceinline__ void deposit(const TArgs& A, double& dep, float px, float py, float pz, float d) {
+// per-thread deposited energy and number of dose-grid atomics
+struct Dep { double e; uint32_t n; };
+
+__device__ __forceinline__ void deposit(const TArgs& A, Dep& dep, float px, float py, float pz, float d) {
     if (d <= 0.0f) return;                                       // primary.wgsl:103
-    dep += (double)d;
+    dep.e += (double)d;
     float vs = 2.0f * A.box / (float)A.vc;
     int ix = (int)floorf((px + A.box) / vs);
     int iy = (int)floorf((py + A.box) / vs);
@@ -108,6 +111,7 @@ __device__ __forceinline__ void deposit(const TArgs& A, double& dep, float px, f
     int n = (int)A.vc;
     if (ix < 0 || ix >= n || iy < 0 || iy >= n || iz < 0 || iz >= n) return;
     atomicAdd(&A.dose[(uint32_t)((iz * n + iy) * n + ix)], (uint32_t)(d * 100.0f));
+    dep.n++;
 }
 
 __device__ __forceinline__ uint32_t dna_near(const TArgs& A, float px, float py, float pz) {
@@ -283,7 +287,7 @@ struct XS {
 };
 
 // the interaction after the move (primary.wgsl:180-649, secondary.wgsl:167-443)
-__device__ __forceinline__ void interact(const TArgs& A, Blk& b, Particle& q, double& dep, const XS& x) {
+__device__ __forceinline__ void interact(const TArgs& A, Blk& b, Particle& q, Dep& dep, const XS& x) {
     const float* T = b.T;
     float E = q.E;
     float px = q.px, py = q.py, pz = q.pz;
@@ -577,7 +581,7 @@ __device__ __forceinline__ void start_primary(const TArgs& A, Particle& q, uint3
     q.tpath = 0.0f; q.ppath = 0.0f; q.maxr = 0.0f; q.nion = 0; q.nexc = 0;
 }
 
-__device__ __forceinline__ void finish_primary(const TArgs& A, Blk& b, Particle& q, double& dep, uint32_t esc) {
+__device__ __forceinline__ void finish_primary(const TArgs& A, Blk& b, Particle& q, Dep& dep, uint32_t esc) {
     if (esc == 0u && q.E > 0.0f) deposit(A, dep, q.px, q.py, q.pz, q.E);
     float4* r = reinterpret_cast<float4*>(A.results + 8ull * (q.pid - A.pid_base));
     r[0] = make_float4(q.tpath, q.ppath, q.E, __uint_as_float(q.nion));
@@ -588,7 +592,7 @@ __device__ __forceinline__ void finish_primary(const TArgs& A, Blk& b, Particle&
 }
 
 // one warp-iteration of a lane's electron
-__device__ __forceinline__ void lane_step(const TArgs& A, Blk& b, Particle& q, double& dep,
+__device__ __forceinline__ void lane_step(const TArgs& A, Blk& b, Particle& q, Dep& dep,
                                           unsigned long long& nsteps) {
     const float box = A.box;
     if (q.prim) {
@@ -682,7 +686,7 @@ __global__ void __launch_bounds__(TB, 2) k_transport(TArgs A) {
     DevState* S = A.st;
     Particle q;
     q.active = false;
-    double dep = 0.0;
+    Dep dep{0.0, 0u};
     unsigned long long nsteps = 0;
     bool busy = false;
     unsigned sleep_ns = 64;
@@ -792,12 +796,14 @@ __global__ void __launch_bounds__(TB, 2) k_transport(TArgs A) {
     }
     flush_staging(A, b, lane);
     for (int o = 16; o; o >>= 1) {
-        dep += __shfl_xor_sync(0xffffffffu, dep, o);
+        dep.e += __shfl_xor_sync(0xffffffffu, dep.e, o);
+        dep.n += __shfl_xor_sync(0xffffffffu, dep.n, o);
         nsteps += __shfl_xor_sync(0xffffffffu, nsteps, o);
     }
     if (lane == 0) {
-        atomicAdd(&S->dep_f64, dep);
+        atomicAdd(&S->dep_f64, dep.e);
         atomicAdd(&S->steps, nsteps);
+        atomicAdd(&cnt[D_DOSE], dep.n);
     }
     __syncthreads();
     if (threadIdx.x < 24 && cnt[threadIdx.x]) {

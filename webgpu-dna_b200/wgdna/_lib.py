@@ -55,7 +55,9 @@ class TransportStats(C.Structure):
 class IrtResult(C.Structure):
     _fields_ = [("counts", (C.c_double * 5) * 7), ("G", (C.c_double * 5) * 7), ("rxn_counts", C.c_uint64 * 9),
                 ("n_reacted", C.c_uint64), ("n_tracks", C.c_uint64), ("n_pairs", C.c_uint64),
-                ("n_events", C.c_uint64), ("chem_n", C.c_uint64), ("ms", C.c_float),
+                ("n_events", C.c_uint64), ("n_particles", C.c_uint64), ("n_init_events", C.c_uint64),
+                ("chem_n", C.c_uint64), ("ms", C.c_float),
+                ("ms_load", C.c_float), ("ms_pairing", C.c_float), ("ms_events", C.c_float),
                 ("device_error", C.c_uint32)]
 
 
