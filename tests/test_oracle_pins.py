@@ -8,15 +8,21 @@ seeding (helpers.wgsl:188-190, buffers.ts:91-104) with floor(E) as the seed,
 like runAtEnergy.  Statistical pins use 3-sigma bands: the published numbers
 are themselves means over 4096 primaries, so sigma combines both samples.
 """
+import json
 import math
+import os
 
 import numpy as np
 import pytest
 
 import oracle
 
-PUBLISHED = {"csda": 2714.4, "ions": 194.1, "sec_per_pri": 143.2, "G_OH": 4.51, "G_eaq": 3.79, "G_H": 0.79,
-             "G1us": (1.551, 1.407, 0.706, 0.604, 0.468)}
+_W = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                 "reference_outputs.json")))["webgpu_10keV"]
+PUBLISHED = {"csda": _W["tracking"]["csdaNm"], "ions": _W["tracking"]["ionsPerPriPrimaryOnly"],
+             "sec_per_pri": _W["tracking"]["secPerPri"], "G_OH": _W["pre_chemistry"]["G_OH_init"],
+             "G_eaq": _W["pre_chemistry"]["G_eaq_init"], "G_H": _W["pre_chemistry"]["G_H_init"],
+             "G1us": tuple(_W["chemistry_1us"][k] for k in ("G_OH", "G_eaq", "G_H", "G_H2O2", "G_H2"))}
 
 
 @pytest.fixture(scope="module")
