@@ -77,9 +77,16 @@ struct Blk {
     int* stn;
 };
 
+// Out-of-line Philox block for the transport stream: the generator is drawn
+// from many call sites, and one shared copy keeps the kernel's code small
+// enough for the instruction cache.
+__device__ __noinline__ u4 philox_transport(uint32_t blk, uint32_t sub, uint32_t pid, uint32_t k0, uint32_t k1) {
+    return philox(blk, sub, pid, 1u, k0, k1);
+}
+
 __device__ __forceinline__ uint32_t rn(Particle& q, uint32_t k0, uint32_t k1) {
     if (q.ri == 4u) {
-        u4 o = philox(q.blk, q.sub, q.pid, 1u, k0, k1);
+        u4 o = philox_transport(q.blk, q.sub, q.pid, k0, k1);
         q.blk++;
         q.b0 = o.x; q.b1 = o.y; q.b2 = o.z; q.b3 = o.w;
         q.ri = 0;
@@ -101,24 +108,38 @@ __device__ __forceinline__ void put(const TArgs& A, Blk& b, Particle& q, float x
 // per-thread deposited energy and number of dose-grid atomics
 struct Dep { double e; uint32_t n; };
 
+// voxel of (px, py, pz) in the vc^3 dose grid over +-box, or ~0u outside (out of line: 9 call sites)
+__device__ __noinline__ uint32_t dose_voxel(float px, float py, float pz, float box, uint32_t vc) {
+    float vs = 2.0f * box / (float)vc;
+    int ix = (int)floorf((px + box) / vs);
+    int iy = (int)floorf((py + box) / vs);
+    int iz = (int)floorf((pz + box) / vs);
+    int n = (int)vc;
+    if (ix < 0 || ix >= n || iy < 0 || iy >= n || iz < 0 || iz >= n) return ~0u;
+    return (uint32_t)((iz * n + iy) * n + ix);
+}
+
 __device__ __forceinline__ void deposit(const TArgs& A, Dep& dep, float px, float py, float pz, float d) {
     if (d <= 0.0f) return;                                       // primary.wgsl:103
     dep.e += (double)d;
-    float vs = 2.0f * A.box / (float)A.vc;
-    int ix = (int)floorf((px + A.box) / vs);
-    int iy = (int)floorf((py + A.box) / vs);
-    int iz = (int)floorf((pz + A.box) / vs);
-    int n = (int)A.vc;
-    if (ix < 0 || ix >= n || iy < 0 || iy >= n || iz < 0 || iz >= n) return;
-    atomicAdd(&A.dose[(uint32_t)((iz * n + iy) * n + ix)], (uint32_t)(d * 100.0f));
+    uint32_t v = dose_voxel(px, py, pz, A.box, A.vc);
+    if (v == ~0u) return;
+    atomicAdd(&A.dose[v], (uint32_t)(d * 100.0f));
     dep.n++;
 }
 
+// dna_near (primary.wgsl:41-86), out of line (4 call sites)
+__device__ __noinline__ uint32_t dna_near_nc(float px, float py, float pz, uint32_t N, float spacing, float x0,
+                                             float rise, float r_bb);
+
 __device__ __forceinline__ uint32_t dna_near(const TArgs& A, float px, float py, float pz) {
-    if (A.dna_enable == 0u) return 0u;                           // primary.wgsl:41-86
+    if (A.dna_enable == 0u) return 0u;
+    return dna_near_nc(px, py, pz, A.dna_grid_n, A.dna_spacing, A.dna_x0, A.dna_rise, A.dna_r_bb);
+}
+
+__device__ __noinline__ uint32_t dna_near_nc(float px, float py, float pz, uint32_t N, float spacing, float x0,
+                                             float rise, float r_bb) {
     const float r_damage = 0.29f;
-    uint32_t N = A.dna_grid_n;
-    float spacing = A.dna_spacing;
     float grid_off = -((float)(N - 1u) * spacing) * 0.5f;
     float inv_s = 1.0f / spacing;
     int fi = (int)rintf((py - grid_off) * inv_s);
@@ -128,15 +149,14 @@ __device__ __forceinline__ uint32_t dna_near(const TArgs& A, float px, float py,
     float fz = grid_off + (float)fj * spacing;
     float y_rel = py - fy, z_rel = pz - fz;
     float r2 = y_rel * y_rel + z_rel * z_rel;
-    float R_reach = A.dna_r_bb + r_damage;
+    float R_reach = r_bb + r_damage;
     if (r2 > R_reach * R_reach) return 0u;
-    int bp_est = (int)rintf((px - A.dna_x0) / A.dna_rise);
+    int bp_est = (int)rintf((px - x0) / rise);
     int b0 = bp_est - 1 > 0 ? bp_est - 1 : 0;
     int b1 = bp_est + 1;
     const float d_phase = (float)(2.0 * 3.14159265 / 10.5);
-    float r_bb = A.dna_r_bb;
     for (int bb = b0; bb <= b1; ++bb) {
-        float bx = A.dna_x0 + (float)bb * A.dna_rise;
+        float bx = x0 + (float)bb * rise;
         float phi = (float)bb * d_phase;
         float s0z, s0y;
         sincosf_(phi, &s0z, &s0y);
@@ -163,19 +183,40 @@ __device__ __forceinline__ float meesungnoen_sigma(float k) {   // primary.wgsl:
     return fmaxf(r, 0.0f) * 0.6267f;
 }
 
-// Gaussian 3-D displacement, the mu1..mu4 pattern of primary.wgsl:216-220
-__device__ __forceinline__ float3 gauss3(const TArgs& A, Particle& q, float sigma) {
-    float u1 = fmaxf(RF(), 1e-30f);
-    float u2 = RF();
+// Gaussian 3-D displacement, the mu1..mu4 pattern of primary.wgsl:216-220.
+// Out of line (8 call sites); the particle's generator state travels by value.
+struct G3 { float x, y, z; uint32_t blk, ri, b0, b1, b2, b3; };
+
+__device__ __noinline__ G3 gauss3_nc(uint32_t blk, uint32_t ri, uint32_t b0, uint32_t b1, uint32_t b2, uint32_t b3,
+                                     uint32_t sub, uint32_t pid, uint32_t k0, uint32_t k1, float sigma) {
+    G3 g;
+    g.blk = blk; g.ri = ri; g.b0 = b0; g.b1 = b1; g.b2 = b2; g.b3 = b3;
+    float u[4];
+    for (int k = 0; k < 4; ++k) {
+        if (g.ri == 4u) {
+            u4 o = philox_transport(g.blk, sub, pid, k0, k1);
+            g.blk++;
+            g.b0 = o.x; g.b1 = o.y; g.b2 = o.z; g.b3 = o.w;
+            g.ri = 0;
+        }
+        uint32_t v = g.ri == 0 ? g.b0 : g.ri == 1 ? g.b1 : g.ri == 2 ? g.b2 : g.b3;
+        g.ri++;
+        u[k] = u01f(v);
+    }
+    float u1 = fmaxf(u[0], 1e-30f);
     float rr = sqrtf(-2.0f * logf_pos(u1)) * sigma;
     float sn, cs;
-    sincosf_(TWO_PI_F * u2, &sn, &cs);
-    float3 d;
-    d.x = rr * cs; d.y = rr * sn;
-    float u3 = fmaxf(RF(), 1e-30f);
-    float u4 = RF();
-    d.z = sqrtf(-2.0f * logf_pos(u3)) * sigma * cosf_(TWO_PI_F * u4);
-    return d;
+    sincosf_(TWO_PI_F * u[1], &sn, &cs);
+    g.x = rr * cs; g.y = rr * sn;
+    float u3 = fmaxf(u[2], 1e-30f);
+    g.z = sqrtf(-2.0f * logf_pos(u3)) * sigma * cosf_(TWO_PI_F * u[3]);
+    return g;
+}
+
+__device__ __forceinline__ float3 gauss3(const TArgs& A, Particle& q, float sigma) {
+    G3 g = gauss3_nc(q.blk, q.ri, q.b0, q.b1, q.b2, q.b3, q.sub, q.pid, A.k0, A.k1, sigma);
+    q.blk = g.blk; q.ri = g.ri; q.b0 = g.b0; q.b1 = g.b1; q.b2 = g.b2; q.b3 = g.b3;
+    return make_float3(g.x, g.y, g.z);
 }
 
 // H2O+ + eaq -> H2Ovib dissociation channels (primary.wgsl:246-276)
@@ -591,25 +632,17 @@ __device__ __forceinline__ void finish_primary(const TArgs& A, Blk& b, Particle&
     q.active = false;
 }
 
-// one warp-iteration of a lane's electron
+// one warp-iteration of a lane's electron.  Primaries and secondaries share
+// one fly + interact call site, so a warp holding both kinds runs the step
+// code once instead of once per kind.
 __device__ __forceinline__ void lane_step(const TArgs& A, Blk& b, Particle& q, Dep& dep,
                                           unsigned long long& nsteps) {
     const float box = A.box;
-    if (q.prim) {
+    const bool prim = q.prim;
+    const bool out = fabsf(q.px) >= box || fabsf(q.py) >= box || fabsf(q.pz) >= box;
+    if (prim) {
         if (q.it >= A.ms || q.E < A.ce) { finish_primary(A, b, q, dep, 0u); return; }
-        if (fabsf(q.px) >= box || fabsf(q.py) >= box || fabsf(q.pz) >= box) { finish_primary(A, b, q, dep, 1u); return; }
-        bool productive = q.E > 12.0f;
-        XS x; float dist;
-        if (!fly(A, b, q, x, dist)) { finish_primary(A, b, q, dep, 0u); return; }
-        nsteps++;
-        q.tpath += dist;
-        if (productive) q.ppath += dist;
-        float rdx = q.px - q.sx, rdy = q.py - q.sy, rdz = q.pz - q.sz;
-        float r = sqrtf(rdx * rdx + rdy * rdy + rdz * rdz);
-        if (r > q.maxr) q.maxr = r;
-        if (fabsf(q.px) >= box || fabsf(q.py) >= box || fabsf(q.pz) >= box) { finish_primary(A, b, q, dep, 1u); return; }
-        interact(A, b, q, dep, x);
-        q.it++;
+        if (out) { finish_primary(A, b, q, dep, 1u); return; }
     } else {
         if (q.it >= A.sec_steps) { q.active = false; return; }
         if (q.E < A.ce) {                                        // secondary.wgsl:100-124
@@ -626,18 +659,32 @@ __device__ __forceinline__ void lane_step(const TArgs& A, Blk& b, Particle& q, D
             q.active = false;
             return;
         }
-        if (fabsf(q.px) >= box || fabsf(q.py) >= box || fabsf(q.pz) >= box) {
+        if (out) {
             atomicAdd(&b.cnt[SS_BOUNDS], 1u);
             q.active = false;
             return;
         }
-        XS x; float dist;
-        if (!fly(A, b, q, x, dist)) { q.active = false; return; }
-        nsteps++;
-        atomicAdd(&b.cnt[SS_STEPS], 1u);
-        interact(A, b, q, dep, x);
-        q.it++;
     }
+    const bool productive = q.E > 12.0f;
+    XS x; float dist;
+    if (!fly(A, b, q, x, dist)) {
+        if (prim) finish_primary(A, b, q, dep, 0u);
+        else q.active = false;
+        return;
+    }
+    nsteps++;
+    if (prim) {
+        q.tpath += dist;
+        if (productive) q.ppath += dist;
+        float rdx = q.px - q.sx, rdy = q.py - q.sy, rdz = q.pz - q.sz;
+        float r = sqrtf(rdx * rdx + rdy * rdy + rdz * rdz);
+        if (r > q.maxr) q.maxr = r;
+        if (fabsf(q.px) >= box || fabsf(q.py) >= box || fabsf(q.pz) >= box) { finish_primary(A, b, q, dep, 1u); return; }
+    } else {
+        atomicAdd(&b.cnt[SS_STEPS], 1u);
+    }
+    interact(A, b, q, dep, x);
+    q.it++;
 }
 
 __device__ __forceinline__ void flush_staging(const TArgs& A, Blk& b, int lane) {
