@@ -66,7 +66,9 @@ struct wgdna_ctx {
     ScoreScratch sc{};
     unsigned long long sc_cap = 0;
     // IRT scratch
-    size_t irt_slots = 0, irt_evslots = 0, irt_hov = 0;
+    size_t irt_slots = 0, irt_evslots = 0, irt_hov = 0, irt_pf_slots = 0;
+    float4* d_pf = nullptr;
+    float* d_tdel = nullptr;
     uint32_t irt_tracks = 0, irt_hcap = 0;
     double *d_px = nullptr, *d_py = nullptr, *d_pz = nullptr, *d_tb = nullptr;
     int8_t* d_sp = nullptr;
@@ -189,7 +191,7 @@ extern "C" void wgdna_destroy(wgdna_ctx* c) {
                     c->d_red, c->d_err, c->d_fy, c->d_fz, c->d_rbb0, c->d_rbb1, c->d_hits, c->d_alive,
                     c->sc.info, c->sc.last_brk, c->sc.cnt0, c->sc.cnt1, c->sc.cs_in, c->sc.base, c->sc.u64,
                     c->sc.fib, c->d_px, c->d_py, c->d_pz, c->d_tb, c->d_sp, c->d_alive8, c->d_lst, c->d_lpos, c->d_evt, c->d_evab,
-                    c->d_hov_t, c->d_hov_ab, c->d_track, c->d_toff, c->d_irt_cnt, c->d_acc_tl, c->d_acc, c->d_maxpid};
+                    c->d_hov_t, c->d_hov_ab, c->d_track, c->d_toff, c->d_irt_cnt, c->d_pf, c->d_tdel, c->d_acc_tl, c->d_acc, c->d_maxpid};
     for (void* p : ptrs) if (p) cudaFree(p);
     for (auto& ev : c->ev) if (ev) cudaEventDestroy(ev);
     if (c->own) cudaStreamDestroy(c->own);
@@ -224,6 +226,7 @@ static IArgs make_iargs(wgdna_ctx* c, uint32_t nseg, uint64_t seed) {
     a.tn = c->d_track; a.th2 = c->d_track + T; a.ttiles = c->d_track + 2 * T; a.tev = c->d_track + 3 * T;
     a.tlc = c->d_track + 4 * T;
     a.toff = c->d_toff;
+    a.pf = c->d_pf; a.tdel = c->d_tdel;
     a.hov_t = c->d_hov_t; a.hov_ab = c->d_hov_ab; a.hcap = c->irt_hcap;
     a.counters = c->d_irt_cnt;
     a.acc_tl = c->d_acc_tl; a.acc = c->d_acc; a.err = c->d_err;
@@ -362,8 +365,13 @@ static int irt_ensure(wgdna_ctx* c, uint32_t nseg, uint64_t rad_n, uint32_t cap)
         c->irt_hov = hov;
     }
     c->irt_hcap = (uint32_t)(hov / irt_warps(c->device));
+    if (slots > c->irt_pf_slots) {
+        TRY(dalloc(&c->d_pf, slots));
+        c->irt_pf_slots = slots;
+    }
     if (nseg > c->irt_tracks) {
         TRY(dalloc(&c->d_track, 10 * (size_t)nseg)); TRY(dalloc(&c->d_toff, (size_t)nseg + 1));
+        TRY(dalloc(&c->d_tdel, (size_t)nseg));
         c->irt_tracks = nseg;
     }
     if (!c->d_irt_cnt) TRY(dalloc(&c->d_irt_cnt, 4));
@@ -531,6 +539,12 @@ static void irt_constants(IrtConst* C) {
     C->sig_h = (17.0 / 18.0) * 2.4 / sqrt(3.0);
     double rcut = 1.45 + 2 * sqrt(8 * 9.46 * 1000);
     C->r_cut2 = rcut * rcut;
+    for (int r = 0; r < 9; ++r) {
+        double sr = C->acc_s[r], ad = C->acc_add[r];
+        C->fa0[r] = (float)(((sr + ad) * (1.0 + 1e-6) + 1e-6) * (1.0 + 1e-7));
+        C->fkb0[r] = (float)((ad * (1.0 + 1e-6) + 1e-6) * (1.0 + 1e-7));
+        C->fk[r] = (float)(sr * C->acc_c[r] * (1.0 + 1e-6) * (1.0 + 1e-6) * (1.0 + 1e-7));
+    }
 }
 
 // ------------------------------------------------------------------ scoring

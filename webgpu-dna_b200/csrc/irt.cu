@@ -70,38 +70,114 @@ __device__ __forceinline__ double erfcx_(double x) {
     return erfcx_pos(x);
 }
 
+// f32 erfcx for z >= 0, used only to bound the f64 value: the reference's
+// Chebyshev form (first 14 coefficients) below 6, the asymptotic series
+// (1 / (z sqrt(pi))) sum (-1)^k (2k-1)!! / (2 z^2)^k to k = 7 above.  Its
+// largest relative error against the f64 form is 3.3e-7 (z on a 1e-5 grid
+// to 200 and log-spaced to 1e8, with a 1-ulp expf).
+__constant__ float c_erfcx_f[14] = {
+    -1.3026537197817094f, 6.4196979235649026e-1f, 1.9476473204185836e-2f, -9.561514786808631e-3f,
+    -9.46595344482036e-4f, 3.66839497852761e-4f, 4.2523324806907e-5f, -2.0278578112534e-5f,
+    -1.624290004647e-6f, 1.303655835580e-6f, 1.5626441722e-8f, -8.5238095915e-8f,
+    6.529054439e-9f, 5.059343495e-9f};
+
+__device__ __forceinline__ float erfcx_f(float z) {
+    if (z >= 6.0f) {
+        float h = 0.5f / (z * z);
+        float s = 1.0f - 13.0f * h;
+        s = 1.0f - 11.0f * h * s; s = 1.0f - 9.0f * h * s; s = 1.0f - 7.0f * h * s;
+        s = 1.0f - 5.0f * h * s; s = 1.0f - 3.0f * h * s; s = 1.0f - h * s;
+        return s * (0.5641895835f / z);
+    }
+    float t = 2.0f / (2.0f + z), ty = 4.0f * t - 2.0f, d = 0.0f, dd = 0.0f;
+    for (int j = 13; j > 0; --j) { float tmp = d; d = ty * d - dd + c_erfcx_f[j]; dd = tmp; }
+    return t * expf(0.5f * (c_erfcx_f[0] + ty * d) - dd);
+}
+
 // SamplePDC (:91-113) for one pair, 32 trials at a time across the warp; the
 // first accepted trial in trial order wins, as in the sequential loop.  Must
 // be called by all 32 lanes with the same arguments.
-__device__ double pdc_warp(uint32_t i, uint32_t j, uint32_t pid, uint32_t k0, uint32_t k1, double a, double b,
+//
+// A trial is accepted when U2 <= lambdax (X <= 2b/a) or U2 M / X <= lambdax
+// (X >= 2b/a), lambdax = e (1 - Q), e = exp(-b^2/X), Q = a sqrt(pi X)
+// erfcx(b/sqrt(X) + a sqrt(X)).  Each trial first brackets the f64 lambdax
+// with f32 arithmetic:
+//   X to 5e-7 relative, so b^2/X to 1e-6 and e to (2e-6 b^2/X + 2e-6);
+//   z to 1e-6 relative, which moves erfcx by at most 1.2e-6 (|d ln erfcx/dz|
+//   <= 1.13 and <= 1/z); with the 3.3e-7 of erfcx_f and the prefactor Q is
+//   known to 2e-5 relative (5x margin), 1 - Q to that plus 1e-6;
+// and decides when U2 (or U2 M against lambdax X) lies outside the bracket
+// with a further 1e-6 (3e-6) margin.  Trials inside the bracket, near
+// X = 2b/a, with e below exp(-80) in case B, z < 0, or a zero draw are
+// evaluated exactly in f64; only the winner's X is computed in f64.
+__device__ __noinline__ double pdc_warp(uint32_t i, uint32_t j, uint32_t pid, uint32_t k0, uint32_t k1, double a, double b,
                            int lane) {
     double p = 2.0 * sqrt(2.0 * b / a);
     double q = 2.0 / sqrt(2.0 * b / a);
     double M = fmax(1.0 / (a * a), 3.0 * b / a);
+    const double pq = p + q * M, thr = p / pq, t2 = 2.0 * b / a;
+    const float pqf = (float)pq, Mf = (float)M, t2f = (float)t2, bbf = (float)(b * b);
+    const float af = (float)a, bf = (float)b;
     for (uint32_t t0 = 0; t0 < 10000; t0 += 32) {
         uint32_t trial = t0 + lane;
-        bool ok = false;
-        double X = 0;
+        int st = 0;                               // 0 rejected, 1 accepted, 2 undecided
+        double U1 = 0, U2 = 0;
         if (trial < 10000) {
             u4 w = philox(i, j, pid, 4u | (trial << 4), k0, k1);
-            double U = u01d(w.x, w.y);
-            if (U < p / (p + q * M)) { double h = U * (p + q * M) / 2; X = h * h; }
-            else { double h = 2 / ((1 - U) * (p + q * M) / M); X = h * h; }
-            U = u01d(w.z, w.w);
-            // lambdax = e * (1 - a sqrt(pi X) erfcx(.)) with a second factor <= 1, so its
-            // computed value never exceeds e: a trial that fails against e alone is
-            // rejected without evaluating erfcx (same decision as the full test)
-            double e = exp_(-b * b / X);
-            double t2 = 2.0 * b / a;
-            double v = U * M / X;
-            if ((X <= t2 && U <= e) || (X >= t2 && v <= e)) {
-                double sqX = sqrt(X);
-                double lambdax = e * (1.0 - a * sqrt(3.141592653589793 * X) * erfcx_(b / sqX + a * sqX));
-                ok = (X <= t2 && U <= lambdax) || (X >= t2 && v <= lambdax);
+            U1 = u01d(w.x, w.y);
+            U2 = u01d(w.z, w.w);
+            st = 2;
+            float xf;
+            if (U1 < thr) { float h = (float)U1 * pqf * 0.5f; xf = h * h; }
+            else { float h = 2.0f * Mf / ((float)(1.0 - U1) * pqf); xf = h * h; }
+            const bool ca = xf < t2f * 0.99999f, cb = xf > t2f * 1.00001f;
+            if (U2 > 0.0 && xf > 0.0f && xf < 3.0e38f && (ca || cb)) {
+                const float argf = bbf / xf;
+                float elo = 0.0f, ehi = 1e-30f;
+                if (argf <= 80.0f) {
+                    const float ef = expf(-argf), re = argf * 2e-6f + 2e-6f;
+                    elo = ef * (1.0f - re); ehi = ef * (1.0f + re);
+                }
+                const float sx = sqrtf(xf);
+                const float zf = bf / sx + af * sx;
+                if (zf >= 0.0f) {
+                    const float Q = af * sqrtf(3.14159265f * xf) * erfcx_f(zf);
+                    const float flo = 1.0f - Q * 1.00002f - 1e-6f, fhi = 1.0f - Q * 0.99998f + 1e-6f;
+                    const double Llo = (double)(elo * fmaxf(flo, 0.0f)) * (1.0 - 1e-6);
+                    const double Lhi = (double)(ehi * fmaxf(fhi, 0.0f)) * (1.0 + 1e-6) + 1e-37;
+                    if (ca) st = U2 <= Llo ? 1 : (U2 > Lhi ? 0 : 2);
+                    else {
+                        const double lhs = U2 * M;
+                        st = lhs <= Llo * (double)xf * (1.0 - 3e-6) ? 1 : (lhs > Lhi * (double)xf * (1.0 + 3e-6) ? 0 : 2);
+                    }
+                }
             }
         }
-        unsigned m = __ballot_sync(0xffffffffu, ok);
-        if (m) return __shfl_sync(0xffffffffu, X, __ffs(m) - 1);
+        if (__any_sync(0xffffffffu, st == 2) && st == 2) {
+            double X;
+            if (U1 < thr) { double h = U1 * pq / 2; X = h * h; }
+            else { double h = 2 / ((1 - U1) * pq / M); X = h * h; }
+            // lambdax <= e: a trial that fails against e alone is rejected
+            // without evaluating erfcx (same decision as the full test)
+            double e = exp_(-b * b / X);
+            double v = U2 * M / X;
+            st = 0;
+            if ((X <= t2 && U2 <= e) || (X >= t2 && v <= e)) {
+                double sqX = sqrt(X);
+                double lambdax = e * (1.0 - a * sqrt(3.141592653589793 * X) * erfcx_(b / sqX + a * sqX));
+                st = ((X <= t2 && U2 <= lambdax) || (X >= t2 && v <= lambdax)) ? 1 : 0;
+            }
+        }
+        unsigned m = __ballot_sync(0xffffffffu, st == 1);
+        if (m) {
+            const int src = __ffs(m) - 1;
+            double X = 0;
+            if (lane == src) {
+                if (U1 < thr) { double h = U1 * pq / 2; X = h * h; }
+                else { double h = 2 / ((1 - U1) * pq / M); X = h * h; }
+            }
+            return __shfl_sync(0xffffffffu, X, src);
+        }
     }
     return -1.0;
 }
@@ -270,6 +346,11 @@ __global__ void __launch_bounds__(IB) k_irt_load(IArgs A) {
         int8_t* sp = A.sp + tb0; uint8_t* alive = A.alive + tb0;
         uint16_t* lst = A.lst + 6 * tb0; uint16_t* lpos = A.lpos + tb0;
         uint32_t n = 0, h2 = 0;
+        float4* pf = A.pf + tb0;
+        // origin of the track's f32 shadow coordinates: its first rad_buf entry
+        const float4 r0 = A.rad[s];
+        const double ox = r0.x, oy = r0.y, oz = r0.z;
+        float mext = 0.0f;
         for (unsigned long long c = s; c < e; c += 32) {
             unsigned long long idx = c + lane;
             bool valid = idx < e;
@@ -309,9 +390,13 @@ __global__ void __launch_bounds__(IB) k_irt_load(IArgs A) {
                 }
                 px[k] = x; py[k] = y; pz[k] = z; tb[k] = 0.0;
                 sp[k] = (int8_t)spc; alive[k] = 1;
+                float fx = (float)(x - ox), fy = (float)(y - oy), fz = (float)(z - oz);
+                pf[k] = make_float4(fx, fy, fz, __int_as_float(spc));
+                mext = fmaxf(mext, fmaxf(fabsf(fx), fmaxf(fabsf(fy), fabsf(fz))));
             }
             n += __popc(m);
         }
+        for (int o = 16; o; o >>= 1) mext = fmaxf(mext, __shfl_xor_sync(FULL, mext, o));
         __syncwarp();
         __threadfence_block();
         uint32_t cnt[6] = {0, 0, 0, 0, 0, 0};
@@ -332,6 +417,8 @@ __global__ void __launch_bounds__(IB) k_irt_load(IArgs A) {
         if (lane == 0) {
             A.tn[p] = n;
             A.th2[p] = h2;
+            // |f32 shadow distance - f64 distance| <= 3.1e-7 * extent; 1e-6 * extent + 1e-4 nm bounds it
+            A.tdel[p] = mext * 1e-6f + 1e-4f;
             A.ttiles[p] = (n + 31) / 32;
             A.tev[p] = 0;
         }
@@ -340,17 +427,119 @@ __global__ void __launch_bounds__(IB) k_irt_load(IArgs A) {
     if (lane == 0 && n_tracks) { atomicAdd(&A.acc[12], n_tracks); atomicAdd(&A.acc[13], n_part); }
 }
 
-// 2) initial pairing (:539-558): one warp per (track, tile of 32 particles);
-//    the 32 particles sit in lane registers, partners j are broadcast 32 at a time
+// Cheap test that a pair may pass the exact acceptance-radius test r2 <= R^2
+// of r_acc: f32 shadow distance r2f (error below del), acceptance word w
+// with U = (w + 0.5) / 2^32 >= Uf.  Never false when the exact test is true:
+//   R = max(s, s c / U) + add  (times 1 + 1e-6, plus 1e-6), so either
+//   rf <= (s + add)(1+1e-6) + 1e-6 + del, or (rf - kb) U <= s c (1+1e-6)^2
+//   with kb = add (1+1e-6) + 1e-6 + del, which holds for Uf <= U as well;
+// both are squared, with a 1e-4 relative margin for the f32 arithmetic.
+__device__ __forceinline__ bool pair_maybe(const IrtConst& C, int ri, float r2f, float del, uint32_t w) {
+    float ta = (C.fa0[ri] + del) * 1.000001f;
+    if (r2f <= ta * ta * 1.0001f) return true;
+    float uf = __uint2float_rd(w) * 2.3283064365386963e-10f;
+    float kb = (C.fkb0[ri] + del) * 1.000001f;
+    float rhs = fmaf(kb, uf, C.fk[ri]);
+    return r2f * uf * uf <= rhs * rhs * 1.0001f;
+}
+
+__device__ __noinline__ u4 philox_accept(uint32_t blk, uint32_t i, uint32_t pid, uint32_t k0, uint32_t k1) {
+    return philox(blk, i, pid, 3u, k0, k1);
+}
+
+// 2) initial pairing (:539-558): one warp per (track, tile of 32 particles).
+//    The tile's particles sit in lane registers as f32 shadows; partners come
+//    32 at a time through shared memory and are read as broadcasts.  The f32
+//    distance settles the R_CUT test and the acceptance prefilter for almost
+//    every pair; the rare candidates (and pairs within rounding of R_CUT) are
+//    queued per warp and redone exactly in f64, 32 at a time, one per lane.
+constexpr int IQ = 64;                   // candidate queue per warp
+
+struct InitTrack {
+    const double *px, *py, *pz;
+    double* ET;
+    uint32_t* EAB;
+    uint32_t* tev;
+    uint32_t ecp, pid;
+};
+
+// exact evaluation of queued candidates [0, cnt): one per lane; returns the
+// reactive pairs inside R_CUT found among the near-R_CUT entries
+__device__ __forceinline__ uint32_t init_batch(const IrtConst& C, const InitTrack& T, const uint32_t* qij,
+                                               const uint32_t* qw, const uint16_t* qk, int cnt, int lane,
+                                               uint32_t k0, uint32_t k1, bool& ev_over) {
+    const unsigned lt = (1u << lane) - 1u;
+    bool acc = false, pdcq = false;
+    double t = 0, pa = 0, pb = 0, pD = 0;
+    uint32_t i = 0, j = 0, np = 0;
+    if (lane < cnt) {
+        const uint32_t ij = qij[lane], k = qk[lane];
+        uint32_t wd = qw[lane];
+        i = ij >> 16; j = ij & 0xffffu;
+        const int kind = (int)(k & 3u), ri = (int)((k >> 2) & 15u);
+        const int si = (int)((k >> 6) & 7u), sj = (int)((k >> 9) & 7u);
+        double dx = T.px[i] - T.px[j], dy = T.py[i] - T.py[j], dz = T.pz[i] - T.pz[j];
+        double r2 = dx * dx + dy * dy + dz * dz;
+        bool inside = true;
+        if (kind == 2) {
+            inside = r2 <= C.r_cut2;
+            if (inside) {
+                np = 1;
+                u4 w4 = philox(j >> 2, i, T.pid, 3u, k0, k1);
+                wd = (j & 3) == 0 ? w4.x : (j & 3) == 1 ? w4.y : (j & 3) == 2 ? w4.z : w4.w;
+            }
+        }
+        if (inside) {
+            double U = u01d32(wd);
+            double R = r_acc(C, ri, U);
+            if (r2 <= R * R) {
+                double D = C.D[si] + C.D[sj];
+                t = sample_pre(C, sqrt(r2), ri, D, U, &pa, &pb);
+                if (t == -2.0) { pdcq = true; pD = D; }
+                else acc = (t >= 0 && t < 1000);
+            }
+        }
+    }
+    unsigned pm = __ballot_sync(FULL, pdcq);
+    while (pm) {
+        int src = __ffs(pm) - 1;
+        pm &= pm - 1;
+        uint32_t qi = __shfl_sync(FULL, i, src), qj = __shfl_sync(FULL, j, src);
+        double qa = __shfl_sync(FULL, pa, src), qb = __shfl_sync(FULL, pb, src);
+        double X = pdc_warp(qi, qj, T.pid, k0, k1, qa, qb, lane);
+        if (lane == src && X > 0) { t = X / pD; acc = t < 1000; }
+    }
+    unsigned m = __ballot_sync(FULL, acc);
+    if (m) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(T.tev, (uint32_t)__popc(m));
+        base = __shfl_sync(FULL, base, 0);
+        uint32_t slot = base + __popc(m & lt);
+        if (acc) {
+            if (slot < T.ecp) { T.ET[slot] = t; T.EAB[slot] = (i << 16) | j; }
+            else ev_over = true;
+        }
+    }
+    return np;
+}
+
 __global__ void __launch_bounds__(IB) k_irt_init(IArgs A) {
     __shared__ IrtConst s_c;
     __shared__ uint32_t s_row[6];
+    __shared__ float4 s_pj[IB / 32][32];
+    __shared__ uint32_t s_qij[IB / 32][IQ], s_qw[IB / 32][IQ];
+    __shared__ uint16_t s_qk[IB / 32][IQ];
     load_consts(&s_c, s_row);
     const IrtConst& C = s_c;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     const unsigned long long nitems = A.toff[A.nseg];
+    const float rcut = (float)sqrt(C.r_cut2);
+    uint32_t* qij = s_qij[wl];
+    uint32_t* qw = s_qw[wl];
+    uint16_t* qk = s_qk[wl];
     unsigned long long n_pairs = 0;
+    bool ev_over = false;
     for (;;) {
         unsigned long long item = 0;
         if (lane == 0) item = atomicAdd(&A.counters[1], 1u);
@@ -359,80 +548,73 @@ __global__ void __launch_bounds__(IB) k_irt_init(IArgs A) {
         uint32_t lo = 0, hi = A.nseg;                 // last p with toff[p] <= item
         while (hi - lo > 1) { uint32_t mid = (lo + hi) >> 1; if (A.toff[mid] <= item) lo = mid; else hi = mid; }
         const uint32_t p = lo;
-        const uint32_t pid = A.pid_base + p;
         const uint32_t n = A.tn[p];
         const uint32_t i0 = 32u * (uint32_t)(item - A.toff[p]);
         const unsigned long long tb0 = tbase(A, p);
-        const double* px = A.px + tb0; const double* py = A.py + tb0; const double* pz = A.pz + tb0;
-        const int8_t* sp = A.sp + tb0;
-        double* ET = A.ev_t + ebase(A, p);
-        uint32_t* EAB = A.ev_ab + ebase(A, p);
-        const uint32_t ecp = ecap(A, p);
-        uint32_t i = i0 + lane;
-        bool hi_ = i < n;
-        double xi = 0, yi = 0, zi = 0, Di = 0;
-        int si = 0;
-        if (hi_) { xi = px[i]; yi = py[i]; zi = pz[i]; si = sp[i]; Di = C.D[si]; }
-        uint32_t row = s_row[si];
+        const float4* pf = A.pf + tb0;
+        const float del = A.tdel[p];
+        const float clo = (rcut - del) * 0.99999f, chi = (rcut + del) * 1.00001f;
+        const float lo2 = clo * clo, hi2 = chi * chi;
+        InitTrack T{A.px + tb0, A.py + tb0, A.pz + tb0, A.ev_t + ebase(A, p), A.ev_ab + ebase(A, p), &A.tev[p],
+                    ecap(A, p), A.pid_base + p};
+        const uint32_t i = i0 + lane;
+        const bool hi_ = i < n;
+        float4 me = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (hi_) me = pf[i];
+        const int si = hi_ ? __float_as_int(me.w) : 0;
+        const uint32_t row = s_row[si];
         uint32_t cblk = 0xffffffffu;
         u4 cw = {0, 0, 0, 0};
-        bool ev_over = false;
+        int qn = 0;
         for (uint32_t j0 = i0; j0 < n; j0 += 32) {
-            uint32_t jl = j0 + lane;
-            double cx = 0, cy = 0, cz = 0;
-            int cs = 0;
-            if (jl < n) { cx = px[jl]; cy = py[jl]; cz = pz[jl]; cs = sp[jl]; }
-            uint32_t kmax = min(32u, n - j0);
+            __syncwarp();
+            if (j0 + lane < n) s_pj[wl][lane] = pf[j0 + lane];
+            __syncwarp();
+            const uint32_t kmax = min(32u, n - j0);
             for (uint32_t kk = 0; kk < kmax; ++kk) {
-                uint32_t j = j0 + kk;
-                double xj = __shfl_sync(FULL, cx, kk), yj = __shfl_sync(FULL, cy, kk), zj = __shfl_sync(FULL, cz, kk);
-                int sj = __shfl_sync(FULL, cs, kk);
-                bool acc = false, pdcq = false;
-                double t = 0, pa = 0, pb = 0, pD = 0;
-                if (hi_ && j > i) {
-                    int ri = (int)((row >> (4 * sj)) & 15u);
-                    if (ri != 15) {
-                        double dx = xi - xj, dy = yi - yj, dz = zi - zj;
-                        double r2 = dx * dx + dy * dy + dz * dz;
-                        if (r2 <= C.r_cut2) {
-                            n_pairs++;
-                            if ((j >> 2) != cblk) { cblk = j >> 2; cw = philox(cblk, i, pid, 3u, A.k0, A.k1); }
-                            uint32_t wd = (j & 3) == 0 ? cw.x : (j & 3) == 1 ? cw.y : (j & 3) == 2 ? cw.z : cw.w;
-                            double U = u01d32(wd);
-                            double R = r_acc(C, ri, U);
-                            if (r2 <= R * R) {
-                                double D = Di + C.D[sj];
-                                t = sample_pre(C, sqrt(r2), ri, D, U, &pa, &pb);
-                                if (t == -2.0) { pdcq = true; pD = D; }
-                                else acc = (t >= 0 && t < 1000);
-                            }
-                        }
-                    }
+                const uint32_t j = j0 + kk;
+                const float4 q = s_pj[wl][kk];
+                const int sj = __float_as_int(q.w);
+                const int ri = (int)((row >> (4 * sj)) & 15u);
+                int kind = 0;                           // 1: candidate, 2: near R_CUT
+                uint32_t wd = 0;
+                if (hi_ && j > i && ri != 15) {
+                    float dx = me.x - q.x, dy = me.y - q.y, dz = me.z - q.z;
+                    float r2f = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                    if (r2f < lo2) {
+                        n_pairs++;
+                        if ((j >> 2) != cblk) { cblk = j >> 2; cw = philox_accept(cblk, i, T.pid, A.k0, A.k1); }
+                        wd = (j & 3) == 0 ? cw.x : (j & 3) == 1 ? cw.y : (j & 3) == 2 ? cw.z : cw.w;
+                        if (pair_maybe(C, ri, r2f, del, wd)) kind = 1;
+                    } else if (r2f <= hi2) kind = 2;
                 }
-                unsigned pm = __ballot_sync(FULL, pdcq);
-                while (pm) {
-                    int src = __ffs(pm) - 1;
-                    pm &= pm - 1;
-                    uint32_t qi = __shfl_sync(FULL, i, src);
-                    double qa = __shfl_sync(FULL, pa, src), qb = __shfl_sync(FULL, pb, src);
-                    double X = pdc_warp(qi, j, pid, A.k0, A.k1, qa, qb, lane);
-                    if (lane == src && X > 0) { t = X / pD; acc = t < 1000; }
-                }
-                unsigned m = __ballot_sync(FULL, acc);
+                const unsigned m = __ballot_sync(FULL, kind != 0);
                 if (m) {
-                    uint32_t base = 0;
-                    if (lane == 0) base = atomicAdd(&A.tev[p], (uint32_t)__popc(m));
-                    base = __shfl_sync(FULL, base, 0);
-                    uint32_t slot = base + __popc(m & lt);
-                    if (acc) {
-                        if (slot < ecp) { ET[slot] = t; EAB[slot] = (i << 16) | j; }
-                        else ev_over = true;
+                    if (kind) {
+                        const int at = qn + __popc(m & lt);
+                        qij[at] = (i << 16) | j;
+                        qw[at] = wd;
+                        qk[at] = (uint16_t)(kind | (ri << 2) | (si << 6) | (sj << 9));
+                    }
+                    qn += __popc(m);
+                    if (qn >= 32) {
+                        __syncwarp();
+                        n_pairs += init_batch(C, T, qij, qw, qk, 32, lane, A.k0, A.k1, ev_over);
+                        __syncwarp();
+                        if (lane < qn - 32) { qij[lane] = qij[32 + lane]; qw[lane] = qw[32 + lane]; qk[lane] = qk[32 + lane]; }
+                        qn -= 32;
+                        __syncwarp();
                     }
                 }
             }
         }
-        if (__any_sync(FULL, ev_over) && lane == 0) atomicOr(A.err, DERR_HEAP);
+        if (qn) {
+            __syncwarp();
+            n_pairs += init_batch(C, T, qij, qw, qk, qn, lane, A.k0, A.k1, ev_over);
+            __syncwarp();
+        }
     }
+    if (__any_sync(FULL, ev_over) && lane == 0) atomicOr(A.err, DERR_HEAP);
     for (int o = 16; o; o >>= 1) n_pairs += __shfl_xor_sync(FULL, n_pairs, o);
     if (lane == 0 && n_pairs) atomicAdd(&A.acc[10], n_pairs);
 }

@@ -12,6 +12,9 @@ struct IrtConst {
     int map[36];
     double D[6];
     double sig_oh, sig_h, sig_eaq, r_cut2;
+    // f32 prefilter bounds of r_acc (irt.cu pair_maybe): (s + add)(1+1e-6) + 1e-6,
+    // add(1+1e-6) + 1e-6 and s c (1+1e-6)^2
+    float fa0[9], fkb0[9], fk[9];
 };
 
 struct IArgs {
@@ -24,6 +27,8 @@ struct IArgs {
     uint8_t* alive;
     uint16_t* lst;                       // 6 lists per track: alive particles of each species
     uint16_t* lpos;                      // position of a particle in its list
+    float4* pf;                          // f32 shadow (x, y, z relative to the track origin, species bits)
+    float* tdel;                         // per track: bound on the shadow's distance error (nm)
     double* ev_t;                        // initial events of each track
     uint32_t* ev_ab;                     // packed (a << 16) | b
     uint32_t *tn, *th2, *ttiles, *tev, *tlc;   // per track: particles, H2 markers, tiles, events, 6 list lengths
