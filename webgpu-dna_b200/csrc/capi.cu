@@ -544,6 +544,9 @@ static void irt_constants(IrtConst* C) {
         C->fa0[r] = (float)(((sr + ad) * (1.0 + 1e-6) + 1e-6) * (1.0 + 1e-7));
         C->fkb0[r] = (float)((ad * (1.0 + 1e-6) + 1e-6) * (1.0 + 1e-7));
         C->fk[r] = (float)(sr * C->acc_c[r] * (1.0 + 1e-6) * (1.0 + 1e-6) * (1.0 + 1e-7));
+        C->fs[r] = (float)(sr * (1.0 + 1e-7));
+        C->fsc[r] = (float)(sr * C->acc_c[r] * (1.0 + 1e-7));
+        C->fadd[r] = (float)(ad * (1.0 + 1e-7));
     }
 }
 

@@ -83,15 +83,16 @@ __constant__ float c_erfcx_f[14] = {
 
 __device__ __forceinline__ float erfcx_f(float z) {
     if (z >= 6.0f) {
-        float h = 0.5f / (z * z);
+        float iz = __frcp_rn(z);
+        float h = 0.5f * iz * iz;
         float s = 1.0f - 13.0f * h;
         s = 1.0f - 11.0f * h * s; s = 1.0f - 9.0f * h * s; s = 1.0f - 7.0f * h * s;
         s = 1.0f - 5.0f * h * s; s = 1.0f - 3.0f * h * s; s = 1.0f - h * s;
-        return s * (0.5641895835f / z);
+        return s * 0.5641895835f * iz;
     }
-    float t = 2.0f / (2.0f + z), ty = 4.0f * t - 2.0f, d = 0.0f, dd = 0.0f;
+    float t = __fdividef(2.0f, 2.0f + z), ty = 4.0f * t - 2.0f, d = 0.0f, dd = 0.0f;
     for (int j = 13; j > 0; --j) { float tmp = d; d = ty * d - dd + c_erfcx_f[j]; dd = tmp; }
-    return t * expf(0.5f * (c_erfcx_f[0] + ty * d) - dd);
+    return t * __expf(0.5f * (c_erfcx_f[0] + ty * d) - dd);
 }
 
 // SamplePDC (:91-113) for one pair, 32 trials at a time across the warp; the
@@ -101,11 +102,13 @@ __device__ __forceinline__ float erfcx_f(float z) {
 // A trial is accepted when U2 <= lambdax (X <= 2b/a) or U2 M / X <= lambdax
 // (X >= 2b/a), lambdax = e (1 - Q), e = exp(-b^2/X), Q = a sqrt(pi X)
 // erfcx(b/sqrt(X) + a sqrt(X)).  Each trial first brackets the f64 lambdax
-// with f32 arithmetic:
-//   X to 5e-7 relative, so b^2/X to 1e-6 and e to (2e-6 b^2/X + 2e-6);
+// with f32 arithmetic (the fast reciprocal, rsqrt, divide and exp2
+// instructions, 2 ulp each; ex2 adds |x| 8.6e-8 for exp(x)):
+//   X to 7e-7 relative, so b^2/X to 1.7e-6 and e to (4e-6 b^2/X + 2e-6);
 //   z to 1e-6 relative, which moves erfcx by at most 1.2e-6 (|d ln erfcx/dz|
-//   <= 1.13 and <= 1/z); with the 3.3e-7 of erfcx_f and the prefactor Q is
-//   known to 2e-5 relative (5x margin), 1 - Q to that plus 1e-6;
+//   <= 1.13 and <= 1/z); with the 3.3e-7 of erfcx_f (8e-7 with the fast
+//   exp) the prefactor Q is known to 4e-6, taken as 2e-5, 1 - Q to that
+//   plus 1e-6;
 // and decides when U2 (or U2 M against lambdax X) lies outside the bracket
 // with a further 1e-6 (3e-6) margin.  Trials inside the bracket, near
 // X = 2b/a, with e below exp(-80) in case B, z < 0, or a zero draw are
@@ -129,19 +132,20 @@ __device__ __noinline__ double pdc_warp(uint32_t i, uint32_t j, uint32_t pid, ui
             st = 2;
             float xf;
             if (U1 < thr) { float h = (float)U1 * pqf * 0.5f; xf = h * h; }
-            else { float h = 2.0f * Mf / ((float)(1.0 - U1) * pqf); xf = h * h; }
+            else { float h = __fdividef(2.0f * Mf, (float)(1.0 - U1) * pqf); xf = h * h; }
             const bool ca = xf < t2f * 0.99999f, cb = xf > t2f * 1.00001f;
-            if (U2 > 0.0 && xf > 0.0f && xf < 3.0e38f && (ca || cb)) {
-                const float argf = bbf / xf;
+            if (U2 > 0.0 && xf > 1e-30f && xf < 1.0e30f && (ca || cb)) {
+                const float rs = rsqrtf(xf);
+                const float argf = bbf * rs * rs;
                 float elo = 0.0f, ehi = 1e-30f;
                 if (argf <= 80.0f) {
-                    const float ef = expf(-argf), re = argf * 2e-6f + 2e-6f;
+                    const float ef = __expf(-argf), re = argf * 4e-6f + 2e-6f;
                     elo = ef * (1.0f - re); ehi = ef * (1.0f + re);
                 }
-                const float sx = sqrtf(xf);
-                const float zf = bf / sx + af * sx;
+                const float sx = xf * rs;
+                const float zf = bf * rs + af * sx;
                 if (zf >= 0.0f) {
-                    const float Q = af * sqrtf(3.14159265f * xf) * erfcx_f(zf);
+                    const float Q = af * 1.7724539f * sx * erfcx_f(zf);
                     const float flo = 1.0f - Q * 1.00002f - 1e-6f, fhi = 1.0f - Q * 0.99998f + 1e-6f;
                     const double Llo = (double)(elo * fmaxf(flo, 0.0f)) * (1.0 - 1e-6);
                     const double Lhi = (double)(ehi * fmaxf(fhi, 0.0f)) * (1.0 + 1e-6) + 1e-37;
@@ -619,6 +623,93 @@ __global__ void __launch_bounds__(IB) k_irt_init(IArgs A) {
     if (lane == 0 && n_pairs) atomicAdd(&A.acc[10], n_pairs);
 }
 
+__device__ __noinline__ u4 philox_pair(uint32_t id, uint32_t jj, uint32_t pid, uint32_t k0, uint32_t k1) {
+    return philox(id, jj, pid, 5u, k0, k1);
+}
+
+// the product being re-paired (uniform over the warp)
+struct ProdCtx {
+    const double *px, *py, *pz, *tb;
+    double nx, ny, nz, et, Di;
+    uint32_t id, pid, k0, k1;
+};
+
+// Exact pairWithAlive step (:430-465) for queued partners [0, cnt), one per
+// lane: Brownian sync of the partner by sqrt(2 D_j dt) (skipped when the
+// Box-Muller radius bound shows it cannot come within r_acc), R_CUT, then
+// sampleIRT; accepted events go to the warp's heap.  Returns true when the
+// heap overflowed.
+__device__ __forceinline__ bool prod_batch(const IrtConst& C, const ProdCtx& P, const uint32_t* pq, int cnt, int lane,
+                                        const Heap& H, uint32_t& hn, uint32_t hcap) {
+    bool acc = false, pdcq = false, over = false;
+    double ta = 0, pa = 0, pb = 0, pD = 0;
+    uint32_t jj = 0;
+    if (lane < cnt) {
+        const uint32_t e = pq[lane];
+        jj = e & 0xffffu;
+        const int r2i = (int)((e >> 16) & 15u), s2 = (int)(e >> 20);
+        const double Dj = C.D[s2];
+        const double dt = P.et - P.tb[jj];
+        double xj = P.px[jj], yj = P.py[jj], zj = P.pz[jj];
+        const u4 q0 = philox(P.id, jj, P.pid, 5u, P.k0, P.k1);
+        const double U = u01d32(q0.w);
+        const double R = r_acc(C, r2i, U);
+        bool need = true;
+        if (dt > 0) {
+            double sig = sqrt(2.0 * Dj * dt);
+            // |gaussian 3-vector| <= sqrt(sum -2 ln u1_k) (Box-Muller radius), with margin
+            float l0 = -2.0f * __logf((float)u01d32(q0.x));
+            float l1 = -2.0f * __logf((float)u01d32(q0.y));
+            float l2 = -2.0f * __logf((float)u01d32(q0.z));
+            double B = (double)sqrtf((l0 + l1 + l2) * 1.0001f) + 1e-4;
+            double ex = P.nx - xj, ey = P.ny - yj, ez = P.nz - zj;
+            double dist = sqrt(ex * ex + ey * ey + ez * ez);
+            if (dist - sig * B > R) need = false;
+            if (need) {
+                u4 q1 = philox(P.id, jj, P.pid, 5u | (1u << 4), P.k0, P.k1);
+                double g0 = sqrt(-2 * log_(u01d32(q0.x) + 1e-30)) * cos_(6.2831853 * u01d32(q1.x));
+                double g1 = sqrt(-2 * log_(u01d32(q0.y) + 1e-30)) * cos_(6.2831853 * u01d32(q1.y));
+                double g2 = sqrt(-2 * log_(u01d32(q0.z) + 1e-30)) * cos_(6.2831853 * u01d32(q1.z));
+                xj += g0 * sig; yj += g1 * sig; zj += g2 * sig;
+            }
+        }
+        if (need) {
+            double dx = P.nx - xj, dy = P.ny - yj, dz = P.nz - zj;
+            double r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 <= C.r_cut2) {
+                double D = P.Di + Dj;
+                double t = sample_pre(C, sqrt(r2), r2i, D, U, &pa, &pb);
+                if (t == -2.0) { pdcq = true; pD = D; }
+                else if (t >= 0) { ta = P.et + t; acc = ta < 1000; }
+            }
+        }
+    }
+    unsigned pm = __ballot_sync(FULL, pdcq);
+    while (pm) {
+        int src = __ffs(pm) - 1;
+        pm &= pm - 1;
+        uint32_t qj = __shfl_sync(FULL, jj, src);
+        double qa = __shfl_sync(FULL, pa, src), qb = __shfl_sync(FULL, pb, src);
+        double X = pdc_warp(P.id, qj, P.pid, P.k0, P.k1, qa, qb, lane);
+        if (lane == src && X > 0) { ta = P.et + X / pD; acc = ta < 1000; }
+    }
+    unsigned m = __ballot_sync(FULL, acc);
+    while (m) {
+        int src = __ffs(m) - 1;
+        m &= m - 1;
+        double tt = __shfl_sync(FULL, ta, src);
+        uint32_t pj = __shfl_sync(FULL, jj, src);
+        if (lane == 0) {
+            if (hn < HS + hcap) {
+                uint32_t a = pj < P.id ? pj : P.id, bq = pj < P.id ? P.id : pj;
+                heap_push(H, hn, tt, (a << 16) | bq);
+            } else over = true;
+        }
+    }
+    hn = __shfl_sync(FULL, hn, 0);
+    return __any_sync(FULL, over);
+}
+
 // 3) events (:566-660): sort the initial events, then pop in (t, i, j) order
 //    merged with a heap of product events; one warp per track
 __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
@@ -626,12 +717,14 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
     __shared__ double s_ht[IB / 32][HS];
     __shared__ uint32_t s_hab[IB / 32][HS];
     __shared__ int s_lc[IB / 32][6];
+    __shared__ uint32_t s_pq[IB / 32][IQ];
     __shared__ IrtConst s_c;
     __shared__ uint32_t s_row[6];
     load_consts(&s_c, s_row);
     const IrtConst& C = s_c;
     const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
     const uint32_t gw = blockIdx.x * (IB / 32) + wl;
+    uint32_t* pq = s_pq[wl];
     for (int k = lane; k < 35; k += 32) s_tl[wl][k] = 0.0;
     int* lc = s_lc[wl];
     Heap H{s_ht[wl], s_hab[wl], A.hov_t + (size_t)gw * A.hcap, A.hov_ab + (size_t)gw * A.hcap};
@@ -654,6 +747,10 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
         double* ET = A.ev_t + ebase(A, p);
         uint32_t* EAB = A.ev_ab + ebase(A, p);
         const uint32_t nev = A.tev[p];
+        float4* pf = A.pf + tb0;
+        const float del = A.tdel[p];
+        const float4 org = A.rad[A.seg_off[p]];
+        const double ox = org.x, oy = org.y, oz = org.z;
         uint32_t cnt[6];
         for (int q = 0; q < 6; ++q) cnt[q] = A.tlc[6 * p + q];
         if (lane < 6) lc[lane] = (int)cnt[lane];
@@ -739,9 +836,11 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
                 if (np_ == 1) { nx = mx; ny = my; nz = mz; }
                 else if (pp == 0) { nx = xa; ny = ya; nz = za; }
                 else { nx = xb; ny = yb; nz = zb; }
+                const float nsx = (float)(nx - ox), nsy = (float)(ny - oy), nsz = (float)(nz - oz);
                 if (lane == 0) {
                     px[id] = nx; py[id] = ny; pz[id] = nz; tb[id] = et;
                     sp[id] = (int8_t)nsp; alive[id] = 1;
+                    pf[id] = make_float4(nsx, nsy, nsz, __int_as_float(nsp));
                     cnt[nsp]++;
                     lst[nsp * cap + lc[nsp]] = (uint16_t)id;
                     lpos[id] = (uint16_t)lc[nsp];
@@ -750,80 +849,61 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
                 ntot++;
                 __syncwarp();
                 __threadfence_block();
-                // pairWithAlive (:430-465) over the alive particles of the species that react with nsp
-                double Di = C.D[nsp];
-                uint32_t rowp = s_row[nsp];
+                // pairWithAlive (:430-465) over the alive particles of the species that react with nsp.
+                // f32 prefilter per partner; the partners it cannot rule out are queued and
+                // evaluated exactly (ProdPair), 32 at a time, one per lane.
+                const double Di = C.D[nsp];
+                const uint32_t rowp = s_row[nsp];
+                int qn = 0;
+                const ProdCtx P{px, py, pz, tb, nx, ny, nz, et, Di, id, pid, A.k0, A.k1};
                 for (int s2 = 0; s2 < 6; ++s2) {
                     const int r2i = (int)((rowp >> (4 * s2)) & 15u);
                     if (r2i == 15) continue;
                     const uint32_t len = (uint32_t)lc[s2];
+                    const float Djf2 = (float)(2.0 * C.D[s2]);
                     for (uint32_t c0 = 0; c0 < len; c0 += 32) {
-                        uint32_t li = c0 + lane;
-                        uint32_t jj = li < len ? lst[s2 * cap + li] : 0u;
-                        bool cand = li < len && jj != id;
-                        bool acc = false, pdcq = false;
-                        double ta = 0, pa = 0, pb = 0, pD = 0;
+                        const uint32_t li = c0 + lane;
+                        const uint32_t jj = li < len ? lst[s2 * cap + li] : 0u;
+                        const bool cand = li < len && jj != id;
+                        bool maybe = false;
                         if (cand) {
                             n_pairs++;
-                            double Dj = C.D[s2];
-                            double dt = et - tb[jj];
-                            double xj = px[jj], yj = py[jj], zj = pz[jj];
-                            u4 q0 = philox(id, jj, pid, 5u, A.k0, A.k1);
-                            double U = u01d32(q0.w);
-                            double R = r_acc(C, r2i, U);
-                            bool need = true;
+                            const float4 q = pf[jj];
+                            const double dt = et - tb[jj];
+                            const u4 q0 = philox_pair(id, jj, pid, A.k0, A.k1);
+                            const float ex = nsx - q.x, ey = nsy - q.y, ez = nsz - q.z;
+                            const float dlo = (sqrtf(fmaf(ez, ez, fmaf(ey, ey, ex * ex))) - del) * 0.999998f;
+                            // R of r_acc for U >= uf, rounded up
+                            const float uf = __uint2float_rd(q0.w) * 2.3283064365386963e-10f;
+                            const float rhi = (fmaxf(C.fs[r2i], __fdividef(C.fsc[r2i], uf)) + C.fadd[r2i]) * 1.00002f + 1e-6f;
+                            float reach = 0.0f;
                             if (dt > 0) {
-                                double sig = sqrt(2.0 * Dj * dt);
-                                // |gaussian 3-vector| <= sqrt(sum -2 ln u1_k) (Box-Muller radius), with margin
-                                float l0 = -2.0f * __logf((float)u01d32(q0.x));
-                                float l1 = -2.0f * __logf((float)u01d32(q0.y));
-                                float l2 = -2.0f * __logf((float)u01d32(q0.z));
-                                double B = (double)sqrtf((l0 + l1 + l2) * 1.0001f) + 1e-4;
-                                double ex = nx - xj, ey = ny - yj, ez = nz - zj;
-                                double dist = sqrt(ex * ex + ey * ey + ez * ez);
-                                if (dist - sig * B > R) need = false;
-                                if (need) {
-                                    u4 q1 = philox(id, jj, pid, 5u | (1u << 4), A.k0, A.k1);
-                                    double g0 = sqrt(-2 * log_(u01d32(q0.x) + 1e-30)) * cos_(6.2831853 * u01d32(q1.x));
-                                    double g1 = sqrt(-2 * log_(u01d32(q0.y) + 1e-30)) * cos_(6.2831853 * u01d32(q1.y));
-                                    double g2 = sqrt(-2 * log_(u01d32(q0.z) + 1e-30)) * cos_(6.2831853 * u01d32(q1.z));
-                                    xj += g0 * sig; yj += g1 * sig; zj += g2 * sig;
-                                }
+                                const float l0 = -2.0f * __logf((float)u01d32(q0.x));
+                                const float l1 = -2.0f * __logf((float)u01d32(q0.y));
+                                const float l2 = -2.0f * __logf((float)u01d32(q0.z));
+                                const float Bf = sqrtf((l0 + l1 + l2) * 1.0001f);
+                                reach = sqrtf((float)(Djf2 * dt)) * 1.00001f * (Bf + 1e-4f);
                             }
-                            if (need) {
-                                double dx = nx - xj, dy = ny - yj, dz = nz - zj;
-                                double r2 = dx * dx + dy * dy + dz * dz;
-                                if (r2 <= C.r_cut2) {
-                                    double D = Di + Dj;
-                                    double t = sample_pre(C, sqrt(r2), r2i, D, U, &pa, &pb);
-                                    if (t == -2.0) { pdcq = true; pD = D; }
-                                    else if (t >= 0) { ta = et + t; acc = ta < 1000; }
-                                }
-                            }
+                            maybe = !(dlo - reach > rhi);
                         }
-                        unsigned pm = __ballot_sync(FULL, pdcq);
-                        while (pm) {
-                            int src = __ffs(pm) - 1;
-                            pm &= pm - 1;
-                            uint32_t qj = __shfl_sync(FULL, jj, src);
-                            double qa = __shfl_sync(FULL, pa, src), qb = __shfl_sync(FULL, pb, src);
-                            double X = pdc_warp(id, qj, pid, A.k0, A.k1, qa, qb, lane);
-                            if (lane == src && X > 0) { ta = et + X / pD; acc = ta < 1000; }
-                        }
-                        unsigned m = __ballot_sync(FULL, acc);
-                        while (m) {
-                            int src = __ffs(m) - 1;
-                            m &= m - 1;
-                            double tt = __shfl_sync(FULL, ta, src);
-                            uint32_t pj = __shfl_sync(FULL, jj, src);
-                            if (lane == 0) {
-                                if (hn < HS + A.hcap) {
-                                    uint32_t a = pj < id ? pj : id, bq = pj < id ? id : pj;
-                                    heap_push(H, hn, tt, (a << 16) | bq);
-                                } else heap_over = true;
+                        const unsigned m = __ballot_sync(FULL, maybe);
+                        if (m) {
+                            if (maybe) pq[qn + __popc(m & ((1u << lane) - 1u))] = jj | ((uint32_t)r2i << 16) | ((uint32_t)s2 << 20);
+                            qn += __popc(m);
+                            if (qn >= 32) {
+                                __syncwarp();
+                                heap_over |= prod_batch(C, P, pq, 32, lane, H, hn, A.hcap);
+                                __syncwarp();
+                                if (lane < qn - 32) pq[lane] = pq[32 + lane];
+                                qn -= 32;
+                                __syncwarp();
                             }
                         }
                     }
+                }
+                if (qn) {
+                    __syncwarp();
+                    heap_over |= prod_batch(C, P, pq, qn, lane, H, hn, A.hcap);
                 }
                 __syncwarp();
                 __threadfence_block();

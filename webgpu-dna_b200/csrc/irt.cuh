@@ -15,6 +15,7 @@ struct IrtConst {
     // f32 prefilter bounds of r_acc (irt.cu pair_maybe): (s + add)(1+1e-6) + 1e-6,
     // add(1+1e-6) + 1e-6 and s c (1+1e-6)^2
     float fa0[9], fkb0[9], fk[9];
+    float fs[9], fsc[9], fadd[9];        // acc_s, acc_s * acc_c, acc_add rounded up to f32
 };
 
 struct IArgs {
