@@ -337,6 +337,151 @@ def run_native(args, ws, rank, local):
     ctx.close()
 
 
+def _irt_alg_bytes(ir):
+    """Algorithmic bytes of the dominant IRT kernel (species read once, events written / read once)."""
+    if ir.ms_pairing >= ir.ms_events:
+        return "k_irt_init", ir.ms_pairing, 25 * ir.n_particles + 12 * ir.n_init_events
+    return "k_irt_loop", ir.ms_events, 12 * ir.n_init_events + 25 * ir.n_particles + \
+        24 * max(ir.n_events - ir.n_init_events, 0)
+
+
+def run_track(args):
+    """Single synthetic 10 keV-like track (510 spurs x 6 species, 2.7 um walk) through
+    the IRT to 1 us: rad_buf from pinned host memory, counts back to the host."""
+    import ctypes as C
+    import numpy as np
+    import torch
+    import oracle
+    import wgdna
+    from wgdna import _lib, synthetic
+    L = _lib.lib()
+    ctx = wgdna.Context(max_primaries=16, max_rad=1_000_000, max_sec=100_000)
+    rad = synthetic.synthetic_track()
+    rad_h = torch.from_numpy(rad).pin_memory()
+    ir = _lib.IrtResult()
+
+    def step():
+        _lib.check("wgdna_run_irt", L.wgdna_run_irt(ctx.h, C.c_void_p(rad_h.data_ptr()), rad.shape[0], 1, 1e4, 1,
+                                                    C.byref(ir)))
+    for _ in range(args.warmup):
+        step()
+    dev_ms, kern = [], []
+    with Clocks(0) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step()
+            dev_ms.append(ir.ms)
+            kern.append(_irt_alg_bytes(ir))
+        wall = time.perf_counter() - t0
+    ms = sum(dev_ms) / len(dev_ms)
+    name, kms, alg = kern[-1]
+    pk = peaks()
+    nthreads = 1
+    t0 = time.perf_counter()
+    reps = 3
+    for _ in range(reps):
+        oracle.irt(rad, 1, 1e4, seed=1, nthreads=nthreads)
+    cpu = reps / (time.perf_counter() - t0)
+    line = {"metric": "single-track IRT to 1 us (2550 species)", "value": 1000.0 / ms, "unit": "tracks/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "none", "vs_baseline": None, "dtype": "f64 IRT", "data": "synthetic",
+            "config": {"workload": "one synthetic track: 510 spurs of OH, e-aq, H3O+, H, H2, OH- "
+                                   "(sigma U[1,2] nm) on a 2.7 um random walk, Philox key 1; IRT to 1 us",
+                       "species": synthetic.tracked_species(rad), "l2": "input far below L2 (one track)"},
+            "e2e": {"value": args.steps / wall, "unit": "tracks/s", "h2d_bytes_per_step": int(rad.nbytes),
+                    "d2h_bytes_per_step": C.sizeof(ir)},
+            "gpu_launches": 9 * (args.steps),
+            "roofline": {"bound": "hbm", "kernel": name, "achieved": alg / (kms / 1000.0) / 1e9,
+                         "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": alg / (kms / 1000.0) / 1e9 / pk["hbm_gbs"],
+                         "traffic": None},
+            "clocks": clk.summary(),
+            "work": {"pairs": int(ir.n_pairs), "events": int(ir.n_events), "reacted": int(ir.n_reacted)},
+            "cpu_baseline": {"value": cpu, "unit": "tracks/s", "cores": nthreads, "kind": "port",
+                             "sample": "the same track, oracle IRT on one thread (the reference worker is "
+                                       "single-threaded)"}}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+MIXED_N = 65536
+
+
+def run_mixed(args):
+    """65,536 primaries, energies log-uniform over 100 eV - 30 keV, in one transport
+    launch, then the IRT over all tracks (species counts from a few to ~4000)."""
+    import ctypes as C
+    import numpy as np
+    import oracle
+    import wgdna
+    from wgdna import _lib, synthetic
+    L = _lib.lib()
+    N = args.np if args.np != NP else MIXED_N
+    E = synthetic.mixed_energies(N)
+    ctx = wgdna.Context(max_primaries=N, max_rad=max(N * 1100, 1_000_000), max_sec=max(N * 130, 100_000))
+    import torch
+    E_h = torch.from_numpy(E).pin_memory()
+    p = wgdna.transport_params(N, 10000.0, 15000.0, 7.5, seed=args.seed, dna_enable=0)
+    p.E_per_primary = E_h.data_ptr()
+    st, ir = _lib.TransportStats(), _lib.IrtResult()
+    Emean = float(np.mean(E.astype(np.float64)))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+
+    def step():
+        _lib.check("wgdna_transport", L.wgdna_transport(ctx.h, C.byref(p), C.byref(st)))
+        _lib.check("wgdna_irt", L.wgdna_irt(ctx.h, st.n_therm, Emean, args.seed + 1, C.byref(ir)))
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    kt, ki = [], []
+    with Clocks(0) as clk:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(k))
+                ev[k][0].record(stream)
+            step()
+            with torch.cuda.stream(stream):
+                ev[k][1].record(stream)
+            kt.append(st.ms_transport)
+            ki.append(_irt_alg_bytes(ir))
+        torch.cuda.synchronize()
+    tot = sum(a.elapsed_time(b) for a, b in ev)
+    value = N * args.steps / (tot / 1000.0)
+    pk = peaks()
+    name, kms, alg = ki[-1]
+    R, S, D = st.rad_n_stored, st.sec_n, st.dbg[5]
+    if sum(kt) / len(kt) > kms:
+        name, kms, alg = "k_transport", sum(kt) / len(kt), 16 * R + 96 * S + 32 * N + 4 * D
+    sample = 1024
+    nthreads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    o = oracle.transport(sample, 10000.0, seed=7, rng_mode=0, dna_enable=0, E_per_primary=E[:sample],
+                         nthreads=nthreads)
+    nth = int((o["results"].view(np.uint32).reshape(-1, 8)[:, 5] == 0).sum())
+    oracle.irt(o["rad"], nth, Emean, seed=7, nthreads=nthreads)
+    cpu = sample / (time.perf_counter() - t0)
+    line = {"metric": "mixed-energy primaries/s (transport+IRT)", "value": value, "unit": "primaries/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 transport / f64 IRT",
+            "data": "synthetic",
+            "config": {"workload": f"{N} primaries, E log-uniform 100 eV - 30 keV (Philox key 3), one transport "
+                                   "launch, IRT to 1 us over all tracks", "np": N,
+                       "l2": "256 MB write between timed steps"},
+            "stage_ms": {"transport": sum(kt) / len(kt), "irt_init": ir.ms_pairing, "irt_loop": ir.ms_events},
+            "roofline": {"bound": "hbm", "kernel": name, "achieved": alg / (kms / 1000.0) / 1e9,
+                         "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": alg / (kms / 1000.0) / 1e9 / pk["hbm_gbs"],
+                         "traffic": None},
+            "clocks": clk.summary(),
+            "work": {"rad_n": int(R), "sec_n": int(S), "tracks": int(ir.n_tracks), "irt_species": int(ir.n_particles),
+                     "irt_pairs": int(ir.n_pairs), "irt_events": int(ir.n_events)},
+            "cpu_baseline": {"value": cpu, "unit": "primaries/s", "cores": nthreads, "kind": "port",
+                             "sample": f"first {sample} primaries of the same energy list, oracle transport + IRT"}}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -346,7 +491,13 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--np", type=int, default=NP, help="primaries per GPU per step (4096 = the benchmark)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", choices=["pipeline", "track", "mixed"], default="pipeline",
+                    help="pipeline = 4096 x 10 keV transport+IRT+scoring (the benchmark); track = one "
+                         "synthetic track through the IRT; mixed = 65,536 primaries of mixed energy")
     args = ap.parse_args()
+    if args.workload != "pipeline":
+        (run_track if args.workload == "track" else run_mixed)(args)
+        return
     ws, rank, local = dist_init(args)
     try:
         if args.impl == "reference":

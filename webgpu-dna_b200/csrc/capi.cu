@@ -342,13 +342,13 @@ extern "C" int wgdna_run_transport(wgdna_ctx* c, const wgdna_transport_params* p
 // ------------------------------------------------------------------ Phase C
 static void irt_constants(IrtConst* C);
 
-// Per-track particle slots 2*len + 512 and event slots 8*len + 8192 (the
-// kernels' tbase / ebase), per-warp heap overflow hcap = 4*cap + 4096 with
-// cap = 2*maxlen + 512 the largest track's particle slots.
+// Per-track particle slots 2*len + 64 and event slots 16*len + 2048 (the
+// kernels' tbase / ebase), per-warp heap overflow hcap = 8*cap + 4096 with
+// cap = 2*maxlen + 64 the largest track's particle slots.
 static int irt_ensure(wgdna_ctx* c, uint32_t nseg, uint64_t rad_n, uint32_t cap) {
-    size_t slots = 2 * (size_t)rad_n + 512 * (size_t)nseg;
-    size_t evslots = 8 * (size_t)rad_n + 8192 * (size_t)nseg;
-    uint32_t hcap = cap * 4u + 4096u;
+    size_t slots = 2 * (size_t)rad_n + 64 * (size_t)nseg;
+    size_t evslots = 16 * (size_t)rad_n + 2048 * (size_t)nseg;
+    uint32_t hcap = cap * 8u + 4096u;
     size_t hov = (size_t)irt_warps(c->device) * hcap;
     if (slots > c->irt_slots) {
         TRY(dalloc(&c->d_px, slots)); TRY(dalloc(&c->d_py, slots)); TRY(dalloc(&c->d_pz, slots));
@@ -396,9 +396,9 @@ static int irt_run(wgdna_ctx* c, uint32_t nseg, uint32_t n_therm, double E_eV, u
     WG_CUDA_OK(cudaMemcpyAsync(&maxseg, c->d_red + 2, 8, cudaMemcpyDeviceToHost, s));
     WG_CUDA_OK(cudaStreamSynchronize(s));
     if (maxseg > (1ull << 24)) { wg_set_error("wgdna_irt: track of %llu entries is too large", maxseg); return WGDNA_ERR_CAPACITY; }
-    uint32_t cap = (uint32_t)(2 * maxseg + 512);
+    uint32_t cap = (uint32_t)(2 * maxseg + 64);
     if (cap > 65535u) {
-        wg_set_error("wgdna_irt: a track of %llu entries exceeds the 32,511-entry limit of the event encoding", maxseg);
+        wg_set_error("wgdna_irt: a track of %llu entries exceeds the 32,735-entry limit of the event encoding", maxseg);
         return WGDNA_ERR_CAPACITY;
     }
     TRY(irt_ensure(c, nseg, chem_n, cap));

@@ -307,14 +307,15 @@ __device__ void warp_sort(double* T, uint32_t* AB, uint32_t n, int lane) {
 constexpr uint32_t FULL = 0xffffffffu;
 
 // Per-track storage (one track = one primary): particle slots at
-// tbase(p) = 2*seg_off[p] + 512*p with capacity 2*len + 512 (len = the
-// track's rad_buf entries), initial-event slots at ebase(p) =
-// 8*seg_off[p] + 8192*p: up to ecap(p) = 4*len + 4096 events, twice that
-// room for the power-of-two padding of the sort.
-__device__ __forceinline__ unsigned long long tbase(const IArgs& A, uint32_t p) { return 2ull * A.seg_off[p] + 512ull * p; }
-__device__ __forceinline__ uint32_t tcap(const IArgs& A, uint32_t p) { return (uint32_t)(2ull * (A.seg_off[p + 1] - A.seg_off[p]) + 512ull); }
-__device__ __forceinline__ unsigned long long ebase(const IArgs& A, uint32_t p) { return 8ull * A.seg_off[p] + 8192ull * p; }
-__device__ __forceinline__ uint32_t ecap(const IArgs& A, uint32_t p) { return (uint32_t)(4ull * (A.seg_off[p + 1] - A.seg_off[p]) + 4096ull); }
+// tbase(p) = 2*seg_off[p] + 64*p with capacity 2*len + 64 (len = the track's
+// rad_buf entries; a track that outgrows it before the reference's CAP sets
+// DERR_TRACK_SIZE), initial-event slots at ebase(p) = 16*seg_off[p] + 2048*p:
+// up to ecap(p) = 8*len + 1024 events (DERR_HEAP beyond), twice that room for
+// the power-of-two padding of the sort.
+__device__ __forceinline__ unsigned long long tbase(const IArgs& A, uint32_t p) { return 2ull * A.seg_off[p] + 64ull * p; }
+__device__ __forceinline__ uint32_t tcap(const IArgs& A, uint32_t p) { return (uint32_t)(2ull * (A.seg_off[p + 1] - A.seg_off[p]) + 64ull); }
+__device__ __forceinline__ unsigned long long ebase(const IArgs& A, uint32_t p) { return 16ull * A.seg_off[p] + 2048ull * p; }
+__device__ __forceinline__ uint32_t ecap(const IArgs& A, uint32_t p) { return (uint32_t)(8ull * (A.seg_off[p + 1] - A.seg_off[p]) + 1024ull); }
 
 __device__ __forceinline__ void load_consts(IrtConst* dst, uint32_t* row) {
     for (int k = threadIdx.x; k < (int)(sizeof(IrtConst) / 4); k += blockDim.x)
@@ -427,6 +428,7 @@ __global__ void __launch_bounds__(IB) k_irt_load(IArgs A) {
             A.tev[p] = 0;
         }
         if (n) { n_tracks++; n_part += n; }
+        if (lane == 0 && n) atomicMax(&A.counters[3], n);
     }
     if (lane == 0 && n_tracks) { atomicAdd(&A.acc[12], n_tracks); atomicAdd(&A.acc[13], n_part); }
 }
@@ -458,6 +460,10 @@ __device__ __noinline__ u4 philox_accept(uint32_t blk, uint32_t i, uint32_t pid,
 //    every pair; the rare candidates (and pairs within rounding of R_CUT) are
 //    queued per warp and redone exactly in f64, 32 at a time, one per lane.
 constexpr int IQ = 64;                   // candidate queue per warp
+#ifndef WG_IRT_PU
+#define WG_IRT_PU 1
+#endif
+constexpr int PU = WG_IRT_PU;            // partner chunks per step of the product re-pairing
 
 struct InitTrack {
     const double *px, *py, *pz;
@@ -725,6 +731,8 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
     const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
     const uint32_t gw = blockIdx.x * (IB / 32) + wl;
     uint32_t* pq = s_pq[wl];
+    // CAP of the reference worker (:405): twice the largest track's species, plus 512
+    const uint32_t capref = 2u * A.counters[3] + 512u;
     for (int k = lane; k < 35; k += 32) s_tl[wl][k] = 0.0;
     int* lc = s_lc[wl];
     Heap H{s_ht[wl], s_hab[wl], A.hov_t + (size_t)gw * A.hcap, A.hov_ab + (size_t)gw * A.hcap};
@@ -751,6 +759,8 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
         const float del = A.tdel[p];
         const float4 org = A.rad[A.seg_off[p]];
         const double ox = org.x, oy = org.y, oz = org.z;
+        // from here on the shadow's w holds the birth time (0 for the initial species)
+        for (uint32_t k = lane; k < n; k += 32) pf[k].w = 0.0f;
         uint32_t cnt[6];
         for (int q = 0; q < 6; ++q) cnt[q] = A.tlc[6 * p + q];
         if (lane < 6) lc[lane] = (int)cnt[lane];
@@ -831,7 +841,8 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
             for (int pp = 0; pp < np_; ++pp) {
                 int nsp = pp == 0 ? C.prod0[ri] : C.prod1[ri];
                 uint32_t id = ntot;
-                if (id >= cap) break;
+                if (id >= capref) break;                 // the reference's CAP (:405, :621)
+                if (id >= cap) { if (lane == 0) atomicOr(A.err, DERR_TRACK_SIZE); break; }
                 double nx, ny, nz;
                 if (np_ == 1) { nx = mx; ny = my; nz = mz; }
                 else if (pp == 0) { nx = xa; ny = ya; nz = za; }
@@ -840,7 +851,7 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
                 if (lane == 0) {
                     px[id] = nx; py[id] = ny; pz[id] = nz; tb[id] = et;
                     sp[id] = (int8_t)nsp; alive[id] = 1;
-                    pf[id] = make_float4(nsx, nsy, nsz, __int_as_float(nsp));
+                    pf[id] = make_float4(nsx, nsy, nsz, (float)et);
                     cnt[nsp]++;
                     lst[nsp * cap + lc[nsp]] = (uint16_t)id;
                     lpos[id] = (uint16_t)lc[nsp];
@@ -856,47 +867,67 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
                 const uint32_t rowp = s_row[nsp];
                 int qn = 0;
                 const ProdCtx P{px, py, pz, tb, nx, ny, nz, et, Di, id, pid, A.k0, A.k1};
+                const float etf = (float)et, dtm = 1e-4f + 1e-6f * etf;
                 for (int s2 = 0; s2 < 6; ++s2) {
                     const int r2i = (int)((rowp >> (4 * s2)) & 15u);
                     if (r2i == 15) continue;
                     const uint32_t len = (uint32_t)lc[s2];
                     const float Djf2 = (float)(2.0 * C.D[s2]);
-                    for (uint32_t c0 = 0; c0 < len; c0 += 32) {
-                        const uint32_t li = c0 + lane;
-                        const uint32_t jj = li < len ? lst[s2 * cap + li] : 0u;
-                        const bool cand = li < len && jj != id;
-                        bool maybe = false;
-                        if (cand) {
-                            n_pairs++;
-                            const float4 q = pf[jj];
-                            const double dt = et - tb[jj];
-                            const u4 q0 = philox_pair(id, jj, pid, A.k0, A.k1);
-                            const float ex = nsx - q.x, ey = nsy - q.y, ez = nsz - q.z;
-                            const float dlo = (sqrtf(fmaf(ez, ez, fmaf(ey, ey, ex * ex))) - del) * 0.999998f;
-                            // R of r_acc for U >= uf, rounded up
-                            const float uf = __uint2float_rd(q0.w) * 2.3283064365386963e-10f;
-                            const float rhi = (fmaxf(C.fs[r2i], __fdividef(C.fsc[r2i], uf)) + C.fadd[r2i]) * 1.00002f + 1e-6f;
-                            float reach = 0.0f;
-                            if (dt > 0) {
-                                const float l0 = -2.0f * __logf((float)u01d32(q0.x));
-                                const float l1 = -2.0f * __logf((float)u01d32(q0.y));
-                                const float l2 = -2.0f * __logf((float)u01d32(q0.z));
-                                const float Bf = sqrtf((l0 + l1 + l2) * 1.0001f);
-                                reach = sqrtf((float)(Djf2 * dt)) * 1.00001f * (Bf + 1e-4f);
-                            }
-                            maybe = !(dlo - reach > rhi);
+                    const float fs = C.fs[r2i], fsc = C.fsc[r2i], fadd = C.fadd[r2i];
+                    const uint16_t* L2 = lst + s2 * cap;
+                    // PU chunks of 32 partners at a time: independent loads and Philox blocks
+                    for (uint32_t c0 = 0; c0 < len; c0 += 32 * PU) {
+                        uint32_t jv[PU];
+                        bool mv[PU];
+#pragma unroll
+                        for (int u = 0; u < PU; ++u) {
+                            const uint32_t li = c0 + 32u * u + lane;
+                            jv[u] = li < len ? L2[li] : 0xffffu;
                         }
-                        const unsigned m = __ballot_sync(FULL, maybe);
-                        if (m) {
-                            if (maybe) pq[qn + __popc(m & ((1u << lane) - 1u))] = jj | ((uint32_t)r2i << 16) | ((uint32_t)s2 << 20);
-                            qn += __popc(m);
-                            if (qn >= 32) {
-                                __syncwarp();
-                                heap_over |= prod_batch(C, P, pq, 32, lane, H, hn, A.hcap);
-                                __syncwarp();
-                                if (lane < qn - 32) pq[lane] = pq[32 + lane];
-                                qn -= 32;
-                                __syncwarp();
+                        float4 qv[PU];
+#pragma unroll
+                        for (int u = 0; u < PU; ++u)
+                            if (jv[u] != 0xffffu) qv[u] = pf[jv[u]];
+#pragma unroll
+                        for (int u = 0; u < PU; ++u) {
+                            const uint32_t jj = jv[u];
+                            mv[u] = false;
+                            if (jj != 0xffffu && jj != id) {
+                                n_pairs++;
+                                const float4 q = qv[u];
+                                const u4 q0 = PU == 1 ? philox_pair(id, jj, pid, A.k0, A.k1) : philox(id, jj, pid, 5u, A.k0, A.k1);
+                                const float ex = nsx - q.x, ey = nsy - q.y, ez = nsz - q.z;
+                                const float dlo = (sqrtf(fmaf(ez, ez, fmaf(ey, ey, ex * ex))) - del) * 0.999998f;
+                                // R of r_acc for U >= uf, rounded up
+                                const float uf = __uint2float_rd(q0.w) * 2.3283064365386963e-10f;
+                                const float rhi = (fmaxf(fs, __fdividef(fsc, uf)) + fadd) * 1.00002f + 1e-6f;
+                                // upper bound of dt = et - t_birth from the f32 birth time (error < dtm)
+                                const float dth = etf - q.w + dtm;
+                                float reach = 0.0f;
+                                if (dth > 0.0f) {
+                                    const float l0 = -2.0f * __logf((float)u01d32(q0.x));
+                                    const float l1 = -2.0f * __logf((float)u01d32(q0.y));
+                                    const float l2 = -2.0f * __logf((float)u01d32(q0.z));
+                                    const float Bf = sqrtf((l0 + l1 + l2) * 1.0001f);
+                                    reach = sqrtf(Djf2 * dth) * 1.00001f * (Bf + 1e-4f);
+                                }
+                                mv[u] = !(dlo - reach > rhi);
+                            }
+                        }
+#pragma unroll
+                        for (int u = 0; u < PU; ++u) {
+                            const unsigned m = __ballot_sync(FULL, mv[u]);
+                            if (m) {
+                                if (mv[u]) pq[qn + __popc(m & ((1u << lane) - 1u))] = jv[u] | ((uint32_t)r2i << 16) | ((uint32_t)s2 << 20);
+                                qn += __popc(m);
+                                if (qn >= 32) {
+                                    __syncwarp();
+                                    heap_over |= prod_batch(C, P, pq, 32, lane, H, hn, A.hcap);
+                                    __syncwarp();
+                                    if (lane < qn - 32) pq[lane] = pq[32 + lane];
+                                    qn -= 32;
+                                    __syncwarp();
+                                }
                             }
                         }
                     }

@@ -28,7 +28,8 @@ struct IArgs {
     uint8_t* alive;
     uint16_t* lst;                       // 6 lists per track: alive particles of each species
     uint16_t* lpos;                      // position of a particle in its list
-    float4* pf;                          // f32 shadow (x, y, z relative to the track origin, species bits)
+    float4* pf;                          // f32 shadow (x, y, z relative to the track origin; w: species bits,
+                                         // in the event kernel the birth time)
     float* tdel;                         // per track: bound on the shadow's distance error (nm)
     double* ev_t;                        // initial events of each track
     uint32_t* ev_ab;                     // packed (a << 16) | b
@@ -38,7 +39,7 @@ struct IArgs {
     double* hov_t;
     uint32_t* hov_ab;
     uint32_t hcap;
-    uint32_t* counters;                  // [0] load, [1] init items, [2] loop tracks
+    uint32_t* counters;                  // [0] load, [1] init items, [2] loop tracks, [3] largest track
     double* acc_tl;                      // 35
     unsigned long long* acc;             // [0..8] rxn, 9 reacted, 10 pairs, 11 events, 12 tracks
     uint32_t* err;
