@@ -117,6 +117,14 @@ int wgdna_run_irt(wgdna_ctx *ctx, const float *rad_buf, uint64_t rad_n, uint32_t
                   double E_eV, uint64_t seed, wgdna_irt_result *out);
 /* The same on the rad_buf left in device memory by the last wgdna_transport. */
 int wgdna_irt(wgdna_ctx *ctx, uint32_t n_therm, double E_eV, uint64_t seed, wgdna_irt_result *out);
+/* Per-track G(t) curves (no reference counterpart: the surrogate chemistry
+ * trains on them).  When enabled, every following IRT call records for each
+ * track (primary id - pid_base) the counts of OH, eaq, H, H2O2 and H2 at the
+ * 16 times t_k = 10^(-3 + 0.4 k) ns, k = 0..15, with the checkpoint rule of
+ * irt-worker.js:566-580.  wgdna_irt_curves copies the last call's
+ * n_tracks x 16 x 5 floats (NULL out: only report n_tracks). */
+int wgdna_irt_record_curves(wgdna_ctx *ctx, int enable);
+int wgdna_irt_curves(wgdna_ctx *ctx, float *out, uint64_t cap_tracks, uint64_t *n_tracks);
 /* Per-reaction constants of the 9-reaction table (irt-worker.js:240-279), host
  * only: out[r] = {sigma, sigma_eff, rc, kdif, kact, prob} in nm / nm^3 ns^-1;
  * the worker reports sigma and rc in its rxn_info (irt-worker.js:690-694). */
@@ -160,6 +168,44 @@ int wgdna_cluster_dsb(wgdna_ctx *ctx, const uint8_t *hits, wgdna_dsb_result *out
 /* Direct SSB + DSB clustering of the rad_buf left by the last wgdna_transport
  * (app.ts:182-185 with the worker backend, where indirect scoring is skipped). */
 int wgdna_score(wgdna_ctx *ctx, uint32_t lcg_state, wgdna_ssb_result *ssb, wgdna_dsb_result *dsb);
+
+/* ---------------------------------------------------------------- surrogate */
+/* Learned chemistry (no reference counterpart): an MLP 64 -> 128 -> 128 ->
+ * 128 -> 80 with GELU, bf16 weights and f32 accumulation on the tensor cores,
+ * mapping a track descriptor to the track's G(t) (per 100 eV of the track's
+ * energy) at the 16 curve times of wgdna_irt_curves, species-major within a
+ * time: out[5 k + s], s = OH, eaq, H, H2O2, H2.  The IRT stays the reference
+ * and the judge: the model is trained on the IRT's own curves.
+ *
+ * Parameters (WGDNA_SG_NPARAM floats): W1 [128][64], b1 [128], W2 [128][128],
+ * b2, W3 [128][128], b3, W4 [80][128], b4 [80].  Standardisation
+ * (2*64 + 2*80 floats): input mean, input std, output mean, output std; the
+ * network sees (x - mean) / std and predicts (G - mean) / std. */
+#define WGDNA_SG_IN 64
+#define WGDNA_SG_OUT 80
+#define WGDNA_SG_NPARAM 51664
+/* Descriptors of the tracks (primaries) of the last wgdna_transport, 64 floats
+ * each (layout in webgpu-dna_b200/csrc/surrogate.cu); out may be NULL. */
+int wgdna_track_descriptors(wgdna_ctx *ctx, float *out, uint64_t cap_tracks, uint64_t *n_tracks);
+/* Random (Glorot, seeded) weights, identity standardisation, fresh Adam state. */
+int wgdna_surrogate_init(wgdna_ctx *ctx, uint64_t seed);
+/* Read and/or replace the f32 parameters (either pointer may be NULL). */
+int wgdna_surrogate_params(wgdna_ctx *ctx, float *get, const float *set);
+int wgdna_surrogate_norm(wgdna_ctx *ctx, float *get, const float *set);
+/* Training data: n descriptors (n x 64) and IRT curves as G values (n x 80),
+ * standardised with the current norm and kept on the device. */
+int wgdna_surrogate_load(wgdna_ctx *ctx, const float *X, const float *G, uint64_t n);
+/* Adam (beta 0.9 / 0.999) on the mean squared error of the standardised
+ * outputs, shuffled full batches; losses[epoch] may be NULL. */
+int wgdna_surrogate_train(wgdna_ctx *ctx, uint32_t epochs, uint32_t batch, float lr, uint64_t seed,
+                          float *losses);
+/* Loss and gradient over the first n loaded rows, without an update. */
+int wgdna_surrogate_grad(wgdna_ctx *ctx, uint64_t n, float *grad, double *loss);
+/* G for n host descriptors (X) or, X NULL, for the last descriptors; G n x 80 (may be NULL). */
+int wgdna_surrogate_predict(wgdna_ctx *ctx, const float *X, uint64_t n, float *G);
+/* Descriptors + prediction + energy-weighted sum for the last transport: the
+ * surrogate's G(t) of the whole batch, G[16][5]; ms = device time. */
+int wgdna_surrogate_chemistry(wgdna_ctx *ctx, double *G, float *ms);
 
 /* Direct SSB scoring that allocates nothing.  No counterpart in the reference:
  * it serves callers that cannot call cudaMalloc (a host running under another

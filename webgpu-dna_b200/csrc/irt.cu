@@ -773,7 +773,8 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
         uint32_t ip = 0, hn = 0;
         uint32_t ntot = n;
         double h2c = (double)A.th2[p];
-        int cp = 0;
+        int cp = 0, c16 = 0;
+        float* curve = A.curves ? A.curves + 80ull * p : nullptr;
         bool heap_over = false;
         const double CP[7] = {0.001, 0.01, 0.1, 1, 10, 100, 1000};
         for (;;) {
@@ -794,6 +795,12 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
                         s_tl[wl][cp * 5 + 2] += cnt[2]; s_tl[wl][cp * 5 + 3] += cnt[4];
                         s_tl[wl][cp * 5 + 4] += h2c;
                         cp++;
+                    }
+                    while (curve && c16 < 16 && et >= C.t16[c16]) {
+                        float* c = curve + 5 * c16;
+                        c[0] = (float)cnt[0]; c[1] = (float)cnt[1]; c[2] = (float)cnt[2]; c[3] = (float)cnt[4];
+                        c[4] = (float)h2c;
+                        c16++;
                     }
                 }
             }
@@ -947,6 +954,12 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
                 s_tl[wl][cp * 5 + 2] += cnt[2]; s_tl[wl][cp * 5 + 3] += cnt[4];
                 s_tl[wl][cp * 5 + 4] += h2c;
                 cp++;
+            }
+            while (curve && c16 < 16) {
+                float* c = curve + 5 * c16;
+                c[0] = (float)cnt[0]; c[1] = (float)cnt[1]; c[2] = (float)cnt[2]; c[3] = (float)cnt[4];
+                c[4] = (float)h2c;
+                c16++;
             }
         }
         __syncwarp();

@@ -16,6 +16,7 @@ struct IrtConst {
     // add(1+1e-6) + 1e-6 and s c (1+1e-6)^2
     float fa0[9], fkb0[9], fk[9];
     float fs[9], fsc[9], fadd[9];        // acc_s, acc_s * acc_c, acc_add rounded up to f32
+    double t16[16];                      // per-track curve times 10^(-3 + 0.4 k) ns
 };
 
 struct IArgs {
@@ -42,6 +43,7 @@ struct IArgs {
     uint32_t* counters;                  // [0] load, [1] init items, [2] loop tracks, [3] largest track
     double* acc_tl;                      // 35
     unsigned long long* acc;             // [0..8] rxn, 9 reacted, 10 pairs, 11 events, 12 tracks
+    float* curves;                       // optional: per track 16 x 5 counts (OH, eaq, H, H2O2, H2)
     uint32_t* err;
 };
 

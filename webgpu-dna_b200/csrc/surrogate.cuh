@@ -1,0 +1,79 @@
+// surrogate.cuh -- learned chemistry: track descriptors and a 64-128-128-128-80
+// GELU MLP with bf16 weights and f32 accumulation on the tcgen05 tensor cores.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+
+namespace wg {
+
+constexpr int SG_IN = 64, SG_HID = 128, SG_OUT = 80;
+constexpr int SG_TILE = 128;                 // rows (tracks) per CTA
+// f32 parameter vector: W1 [128][64], b1, W2 [128][128], b2, W3 [128][128], b3, W4 [80][128], b4
+constexpr int SG_OFF_W1 = 0, SG_OFF_B1 = SG_OFF_W1 + SG_HID * SG_IN;
+constexpr int SG_OFF_W2 = SG_OFF_B1 + SG_HID, SG_OFF_B2 = SG_OFF_W2 + SG_HID * SG_HID;
+constexpr int SG_OFF_W3 = SG_OFF_B2 + SG_HID, SG_OFF_B3 = SG_OFF_W3 + SG_HID * SG_HID;
+constexpr int SG_OFF_W4 = SG_OFF_B3 + SG_HID, SG_OFF_B4 = SG_OFF_W4 + SG_OUT * SG_HID;
+constexpr int SG_NPARAM = SG_OFF_B4 + SG_OUT;
+
+// bf16 copies of the weights: W_l as [out][in] and transposed [in][out]
+struct SgWeights {
+    const __nv_bfloat16 *W[4], *WT[4];
+    const float* p;                          // f32 parameters (biases read from here)
+};
+
+struct SgFwdArgs {
+    const float* X;                          // n x 64 standardised inputs
+    const uint32_t* rows;                    // optional gather (batch -> row of X / T)
+    uint32_t n;
+    SgWeights w;
+    float* Y;                                // n x 80 outputs
+    // training: saved activations of the batch (bf16 inputs of each layer, f32 pre-activations)
+    __nv_bfloat16 *H0, *H1, *H2, *H3;
+    float *Z1, *Z2, *Z3;
+    uint32_t* err;
+};
+
+struct SgBwdArgs {
+    const float* T;                          // targets (standardised), rows gathered like X
+    const uint32_t* rows;
+    uint32_t n;                              // batch size
+    SgWeights w;
+    const float* Y;
+    const __nv_bfloat16 *H0, *H1, *H2, *H3;
+    const float *Z1, *Z2, *Z3;
+    float* grad;                             // f32, SG_NPARAM, accumulated with atomics
+    double* loss;                            // sum of squared errors
+    uint32_t* err;
+};
+
+// descriptors of the tracks of a canonical rad_buf
+struct DescArgs {
+    const float4* rad;
+    const unsigned long long* seg_off;
+    uint32_t nseg;
+    const float* E;                          // per-track energy (eV) or null
+    float E0;                                // energy when E is null
+    float* out;                              // nseg x 64
+};
+
+cudaError_t launch_descriptors(const DescArgs& a, cudaStream_t s);
+cudaError_t launch_sg_forward(const SgFwdArgs& a, cudaStream_t s);
+cudaError_t launch_sg_backward(const SgBwdArgs& a, cudaStream_t s);
+// Adam on the f32 parameters, then the bf16 weight copies; zeroes the gradient
+cudaError_t launch_sg_adam(float* p, float* m, float* v, float* grad, float lr, float b1t, float b2t,
+                           __nv_bfloat16* Wcat, __nv_bfloat16* WTcat, cudaStream_t s);
+// bf16 copies of the weights only
+cudaError_t launch_sg_convert(const float* p, __nv_bfloat16* Wcat, __nv_bfloat16* WTcat, cudaStream_t s);
+// standardise rows: out = (in - mean) / std
+cudaError_t launch_sg_standardise(const float* in, float* out, uint64_t n, int dim, const float* mean,
+                                  const float* inv_std, cudaStream_t s);
+// energy-weighted sums of de-standardised outputs: acc[k] += (y * std + mean)[k] * E_track
+cudaError_t launch_sg_reduce(const float* Y, uint32_t n, const float* ymean, const float* ystd, const float* E,
+                             float E0, double* acc, cudaStream_t s);
+
+// offsets of W_l (and WT_l) inside the concatenated bf16 arrays
+constexpr int SG_WOFF[4] = {0, SG_HID * SG_IN, SG_HID * SG_IN + SG_HID * SG_HID, SG_HID * SG_IN + 2 * SG_HID * SG_HID};
+constexpr int SG_WTOTAL = SG_HID * SG_IN + 2 * SG_HID * SG_HID + SG_OUT * SG_HID;
+
+}  // namespace wg

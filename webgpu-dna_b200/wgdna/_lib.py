@@ -21,7 +21,11 @@ EXPORTS = ["wgdna_default_cfg", "wgdna_create", "wgdna_destroy", "wgdna_last_err
            "wgdna_set_stream", "wgdna_transport", "wgdna_transport_copy_out", "wgdna_run_transport",
            "wgdna_run_irt", "wgdna_irt", "wgdna_build_dna_target", "wgdna_set_dna_target",
            "wgdna_score_direct", "wgdna_score_indirect", "wgdna_cluster_dsb", "wgdna_score",
-           "wgdna_score_direct_noalloc", "wgdna_reaction_table"]
+           "wgdna_score_direct_noalloc", "wgdna_reaction_table", "wgdna_irt_record_curves", "wgdna_irt_curves",
+           "wgdna_track_descriptors", "wgdna_surrogate_init", "wgdna_surrogate_params", "wgdna_surrogate_norm",
+           "wgdna_surrogate_load", "wgdna_surrogate_train", "wgdna_surrogate_grad", "wgdna_surrogate_predict",
+           "wgdna_surrogate_chemistry"]
+SG_IN, SG_OUT, SG_NPARAM = 64, 80, 51664
 
 
 class WgdnaError(RuntimeError):
@@ -112,6 +116,17 @@ def lib():
         "wgdna_reaction_table": (C.c_int, [vp]),
         "wgdna_score_direct_noalloc": (C.c_int, [vp, C.c_uint64, vp, vp, vp, vp, P(DnaInfo), C.c_uint32, vp, vp,
                                                  P(SsbResult)]),
+        "wgdna_irt_record_curves": (C.c_int, [vp, C.c_int]),
+        "wgdna_irt_curves": (C.c_int, [vp, vp, C.c_uint64, P(C.c_uint64)]),
+        "wgdna_track_descriptors": (C.c_int, [vp, vp, C.c_uint64, P(C.c_uint64)]),
+        "wgdna_surrogate_init": (C.c_int, [vp, C.c_uint64]),
+        "wgdna_surrogate_params": (C.c_int, [vp, vp, vp]),
+        "wgdna_surrogate_norm": (C.c_int, [vp, vp, vp]),
+        "wgdna_surrogate_load": (C.c_int, [vp, vp, vp, C.c_uint64]),
+        "wgdna_surrogate_train": (C.c_int, [vp, C.c_uint32, C.c_uint32, C.c_float, C.c_uint64, vp]),
+        "wgdna_surrogate_grad": (C.c_int, [vp, C.c_uint64, vp, P(C.c_double)]),
+        "wgdna_surrogate_predict": (C.c_int, [vp, vp, C.c_uint64, vp]),
+        "wgdna_surrogate_chemistry": (C.c_int, [vp, vp, P(C.c_float)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
