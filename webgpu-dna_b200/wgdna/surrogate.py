@@ -1,0 +1,122 @@
+"""Surrogate chemistry on the host side: training data from the IRT, fitting,
+and the surrogate-or-IRT choice of the chemistry step.
+
+The model (csrc/surrogate.cu) maps a track descriptor (64 floats, computed on
+the device from the track's rad_buf entries) to the track's G(t) at the 16
+curve times t_k = 10^(-3 + 0.4 k) ns for OH, e-aq, H, H2O2 and H2.  Training
+targets are the IRT's own per-track curves (wgdna_irt_curves) divided by the
+track's energy / 100 eV.  The IRT stays the judge: ``chemistry`` falls back
+to it when a batch's descriptors leave the training range.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .dispatch import transport_params
+
+TIMES_NS = 10.0 ** (-3.0 + 0.4 * np.arange(16))
+SPECIES = ("OH", "eaq", "H", "H2O2", "H2")
+
+
+def track_data(ctx, energies, seed, box_nm=15000.0, ce_eV=7.5, irt_seed=None):
+    """One transport + IRT batch: descriptors X (n x 64), per-track G curves
+    (n x 80) and energies of the tracks that hold chemistry species."""
+    L = _lib.lib()
+    E = np.ascontiguousarray(energies, np.float32)
+    n = E.size
+    p = transport_params(n, float(E[0]), box_nm, ce_eV, seed=seed, dna_enable=0)
+    p.E_per_primary = E.ctypes.data
+    st = _lib.TransportStats()
+    _lib.check("wgdna_transport", L.wgdna_transport(ctx.h, C.byref(p), C.byref(st)))
+    X = np.zeros((n, 64), np.float32)
+    k = C.c_uint64()
+    _lib.check("wgdna_track_descriptors", L.wgdna_track_descriptors(ctx.h, _lib.ptr(X), n, C.byref(k)))
+    _lib.check("wgdna_irt_record_curves", L.wgdna_irt_record_curves(ctx.h, 1))
+    ir = _lib.IrtResult()
+    try:
+        _lib.check("wgdna_irt", L.wgdna_irt(ctx.h, st.n_therm, float(E.mean()),
+                                            seed + 1 if irt_seed is None else irt_seed, C.byref(ir)))
+        cv = np.zeros((n, 16, 5), np.float32)
+        _lib.check("wgdna_irt_curves", L.wgdna_irt_curves(ctx.h, _lib.ptr(cv), n, C.byref(k)))
+    finally:
+        L.wgdna_irt_record_curves(ctx.h, 0)
+    G = cv.reshape(n, 80) / (E[:, None] / 100.0)
+    keep = cv[:, 0, :].sum(axis=1) > 0
+    return X[keep], G[keep], E[keep], ir
+
+
+def norm_stats(X, G):
+    xm, xs = X.mean(axis=0), X.std(axis=0)
+    xs = np.where(xs > 1e-6, xs, 1.0)
+    ym, ys = G.mean(axis=0), G.std(axis=0)
+    ys = np.where(ys > 1e-6, ys, 1.0)
+    return np.concatenate([xm, xs, ym, ys]).astype(np.float32)
+
+
+def fit(ctx, X, G, schedule=((60, 2e-3), (30, 5e-4), (10, 1e-4)), batch=1024, seed=0):
+    """Initialise, standardise with the data's statistics and train with Adam
+    through the (epochs, learning rate) stages; returns the loss per epoch."""
+    L = _lib.lib()
+    _lib.check("wgdna_surrogate_init", L.wgdna_surrogate_init(ctx.h, seed))
+    nrm = norm_stats(X, G)
+    _lib.check("wgdna_surrogate_norm", L.wgdna_surrogate_norm(ctx.h, None, _lib.ptr(nrm)))
+    X = np.ascontiguousarray(X, np.float32)
+    G = np.ascontiguousarray(G, np.float32)
+    _lib.check("wgdna_surrogate_load", L.wgdna_surrogate_load(ctx.h, _lib.ptr(X), _lib.ptr(G), X.shape[0]))
+    out = []
+    for k, (epochs, lr) in enumerate(schedule):
+        losses = np.zeros(epochs, np.float32)
+        _lib.check("wgdna_surrogate_train", L.wgdna_surrogate_train(ctx.h, epochs, batch, lr, seed + 7919 * k,
+                                                                    _lib.ptr(losses)))
+        out.append(losses)
+    return np.concatenate(out)
+
+
+def predict(ctx, X):
+    L = _lib.lib()
+    X = np.ascontiguousarray(X, np.float32)
+    G = np.zeros((X.shape[0], 80), np.float32)
+    _lib.check("wgdna_surrogate_predict", L.wgdna_surrogate_predict(ctx.h, _lib.ptr(X), X.shape[0], _lib.ptr(G)))
+    return G
+
+
+def batch_G(G, E):
+    """Energy-weighted G(t) of a batch of tracks (16 x 5), as the IRT normalises."""
+    w = np.asarray(E, np.float64)
+    return (np.asarray(G, np.float64) * w[:, None]).sum(axis=0).reshape(16, 5) / w.sum()
+
+
+def in_range(ctx, X, margin=0.0):
+    """True when every descriptor lies inside the training data's range (per
+    standardised feature, the range the model was fitted on plus a margin)."""
+    L = _lib.lib()
+    nrm = np.zeros(2 * 64 + 2 * 80, np.float32)
+    _lib.check("wgdna_surrogate_norm", L.wgdna_surrogate_norm(ctx.h, _lib.ptr(nrm), None))
+    xm, xs = nrm[:64], nrm[64:128]
+    z = (np.asarray(X) - xm) / xs
+    return bool(np.all(np.abs(z) <= 6.0 + margin))
+
+
+def chemistry(ctx, n_therm, E_eV, seed=1):
+    """G(t) of the last transport from the surrogate (16 x 5), or from the IRT
+    when the batch's descriptors leave the training range: (G, used_surrogate)."""
+    L = _lib.lib()
+    k = C.c_uint64()
+    _lib.check("wgdna_track_descriptors", L.wgdna_track_descriptors(ctx.h, None, 0, C.byref(k)))
+    X = np.zeros((k.value, 64), np.float32)
+    _lib.check("wgdna_track_descriptors", L.wgdna_track_descriptors(ctx.h, _lib.ptr(X), k.value, C.byref(k)))
+    if in_range(ctx, X):
+        G = np.zeros(80, np.float64)
+        ms = C.c_float()
+        _lib.check("wgdna_surrogate_chemistry", L.wgdna_surrogate_chemistry(ctx.h, _lib.ptr(G), C.byref(ms)))
+        return G.reshape(16, 5), True
+    L.wgdna_irt_record_curves(ctx.h, 1)
+    ir = _lib.IrtResult()
+    try:
+        _lib.check("wgdna_irt", L.wgdna_irt(ctx.h, n_therm, E_eV, seed, C.byref(ir)))
+        cv = np.zeros((k.value, 16, 5), np.float32)
+        _lib.check("wgdna_irt_curves", L.wgdna_irt_curves(ctx.h, _lib.ptr(cv), k.value, C.byref(k)))
+    finally:
+        L.wgdna_irt_record_curves(ctx.h, 0)
+    return cv.sum(axis=0) / (n_therm * E_eV / 100.0), False
