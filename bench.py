@@ -482,6 +482,165 @@ def run_mixed(args):
     ctx.close()
 
 
+def _train_surrogate(ctx, batches_per_energy, seed0=100):
+    """IRT curves of batches_per_energy x 4096 tracks at each of 1, 3, 10 keV, then the staged fit."""
+    import numpy as np
+    from wgdna import surrogate as S
+    Xs, Gs = [], []
+    seed = seed0
+    t0 = time.perf_counter()
+    for E in (1000.0, 3000.0, 10000.0):
+        for _ in range(batches_per_energy):
+            X, G, _, _ = S.track_data(ctx, np.full(4096, E, np.float32), seed)
+            seed += 7
+            Xs.append(X); Gs.append(G)
+    X, G = np.concatenate(Xs), np.concatenate(Gs)
+    t1 = time.perf_counter()
+    losses = S.fit(ctx, X, G, schedule=((60, 2e-3), (30, 5e-4), (15, 1e-4)), seed=1)
+    return {"tracks": int(X.shape[0]), "data_s": t1 - t0, "train_s": time.perf_counter() - t1,
+            "loss_first": float(losses[0]), "loss_last": float(losses[-1]), "epochs": int(losses.size)}
+
+
+def _g_errors(gi, gp):
+    import numpy as np
+    rel = np.abs(gp - gi) / np.maximum(np.abs(gi), 1e-12)
+    return float(rel[15].max()), float(rel[gi > 0.05].max())
+
+
+def run_surrogate(args):
+    """The learned chemistry against the IRT it replaces: trained on ~1e5 IRT
+    tracks at 1, 3 and 10 keV, then timed on held-out 4096-track batches
+    (transport outside the timed region; both chemistry paths on the same tracks)."""
+    import ctypes as C
+    import numpy as np
+    import oracle
+    import wgdna
+    from wgdna import _lib, surrogate as S
+    L = _lib.lib()
+    ctx = wgdna.Context(max_primaries=4096, max_rad=8_000_000, max_sec=1_200_000)
+    train = _train_surrogate(ctx, 8)
+    per_E = {}
+    pk = peaks()
+    with Clocks(0) as clk:
+        for E in (1000.0, 3000.0, 10000.0):
+            t_irt, t_sg, errs = [], [], []
+            for k in range(args.warmup + args.steps):
+                Xh, Gh, Eh, ir = S.track_data(ctx, np.full(4096, E, np.float32), 777 + 13 * k + int(E))
+                gi = S.batch_G(Gh, Eh)
+                Gc = np.zeros(80)
+                ms = C.c_float()
+                _lib.check("chem", L.wgdna_surrogate_chemistry(ctx.h, _lib.ptr(Gc), C.byref(ms)))
+                if k >= args.warmup:
+                    t_irt.append(ir.ms)
+                    t_sg.append(ms.value)
+                    errs.append(_g_errors(gi, Gc.reshape(16, 5)))
+            per_E[int(E)] = {"irt_ms": sum(t_irt) / len(t_irt), "surrogate_ms": sum(t_sg) / len(t_sg),
+                             "speedup": sum(t_irt) / sum(t_sg),
+                             "G_err_1us": max(e[0] for e in errs), "G_err_max": max(e[1] for e in errs)}
+    # CPU: the oracle IRT on 256 tracks of a 10 keV batch, all host threads
+    nthreads = os.cpu_count() or 1
+    o = oracle.transport(256, 10000.0, seed=3, rng_mode=0, dna_enable=0, nthreads=nthreads)
+    nth = int((o["results"].view(np.uint32).reshape(-1, 8)[:, 5] == 0).sum())
+    t0 = time.perf_counter()
+    oracle.irt(o["rad"], nth, 10000.0, seed=3, nthreads=nthreads)
+    cpu = 256 / (time.perf_counter() - t0)
+    r10 = per_E[10000]
+    line = {"metric": "surrogate vs IRT chemistry speedup at 10 keV (G error <= 2%)", "value": r10["speedup"],
+            "unit": "x", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": r10["surrogate_ms"], "higher_is_better": True, "scaling": "none", "vs_baseline": None,
+            "dtype": "bf16 weights / f32 accumulate (surrogate), f64 (IRT)", "data": "synthetic",
+            "config": {"workload": "4096-track batches at 1, 3, 10 keV; MLP 64-128-128-128-80 GELU trained on "
+                                   "the IRT's per-track G(t) at 16 times (1 ps - 1 us)", "training": train},
+            "per_energy": per_E,
+            "e2e": {"value": 4096 / (r10["surrogate_ms"] / 1000.0), "unit": "tracks/s",
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 81 * 8},
+            "gpu_launches": 5 * args.steps * 3,
+            "roofline": {"bound": "hbm", "kernel": "k_descriptors", "achieved": None, "peak": pk["hbm_gbs"],
+                         "unit": "GB/s", "frac": None, "traffic": None},
+            "clocks": clk.summary(),
+            "cpu_baseline": {"value": cpu, "unit": "tracks/s", "cores": nthreads, "kind": "port",
+                             "sample": "oracle IRT on 256 tracks of a 10 keV batch (the chemistry the surrogate replaces)"}}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def run_sweep(args):
+    """DNA-damage sweep: primaries at 1, 3 and 10 keV in batches of 4096
+    through transport, the surrogate chemistry (the IRT judging 1 % of the
+    batches) and direct SSB + DSB scoring (10 bp window) on the 21 x 21 fibre
+    grid; yields per Gy and per primary."""
+    import ctypes as C
+    import numpy as np
+    import wgdna
+    from wgdna import _lib, surrogate as S
+    L = _lib.lib()
+    n_per = args.np if args.np != NP else 1_000_000
+    B = 4096
+    ctx = wgdna.Context(max_primaries=B, max_rad=8_000_000, max_sec=1_200_000)
+    train = _train_surrogate(ctx, 8)
+    dna = wgdna.build_dna_target()
+    box = 15000.0
+    mass_kg = ((2 * box * 1e-9) ** 3) * 1000.0
+    rows = {}
+    stream_ms = 0.0
+    with Clocks(0) as clk:
+        for E in (1000.0, 3000.0, 10000.0):
+            nb = (n_per + B - 1) // B
+            st, ssb, dsb = _lib.TransportStats(), _lib.SsbResult(), _lib.DsbResult()
+            ir = _lib.IrtResult()
+            dep = 0.0
+            n_ssb = n_dsb = 0
+            judge = []
+            Gsum = np.zeros(80)
+            ms_tr = ms_sg = ms_sc = 0.0
+            t0 = time.perf_counter()
+            for b in range(nb):
+                n = min(B, n_per - b * B)
+                p = wgdna.transport_params(n, E, box, 7.5, dna=dna, seed=int(E) * 1000 + b, dna_enable=1)
+                p.pid_base = b * B
+                _lib.check("transport", L.wgdna_transport(ctx.h, C.byref(p), C.byref(st)))
+                Gc = np.zeros(80)
+                ms = C.c_float()
+                _lib.check("chem", L.wgdna_surrogate_chemistry(ctx.h, _lib.ptr(Gc), C.byref(ms)))
+                if b % 100 == 50 or nb < 100 and b == nb // 2:                      # the IRT judges 1 %
+                    L.wgdna_irt_record_curves(ctx.h, 1)
+                    _lib.check("irt", L.wgdna_irt(ctx.h, st.n_therm, E, b + 1, C.byref(ir)))
+                    L.wgdna_irt_record_curves(ctx.h, 0)
+                    # 1 ps, 100 ps, 10 ns and 1 us are both IRT checkpoints and curve times
+                    gi = np.array(ir.G)[[0, 2, 4, 6]]
+                    gs = Gc.reshape(16, 5)[[0, 5, 10, 15]]
+                    judge.append(float((np.abs(gs - gi) / np.maximum(gi, 1e-12))[gi > 0.05].max()))
+                _lib.check("score", L.wgdna_score(ctx.h, 0x12345678, C.byref(ssb), C.byref(dsb)))
+                dep += st.dep_eV_f64
+                n_ssb += ssb.ssb
+                n_dsb += dsb.dsb
+                Gsum += Gc * n * E
+                ms_tr += st.ms_transport; ms_sg += ms.value; ms_sc += ssb.ms + dsb.ms
+            wall = time.perf_counter() - t0
+            dose = dep * 1.602e-19 / mass_kg
+            gbp = dna.n_bp * 1e-9
+            rows[int(E)] = {"primaries": n_per, "batches": nb, "dose_Gy": dose,
+                            "SSB_per_primary": n_ssb / n_per, "DSB_per_primary": n_dsb / n_per,
+                            "DSB_per_Gy_Gbp": n_dsb / (dose * gbp) if dose > 0 else 0.0,
+                            "SSB_per_Gy_Gbp": n_ssb / (dose * gbp) if dose > 0 else 0.0,
+                            "G_1us": list(np.round((Gsum / (n_per * E)).reshape(16, 5)[15], 4)),
+                            "irt_judge_max_rel_err": max(judge) if judge else None, "irt_judged_batches": len(judge),
+                            "device_ms": {"transport": ms_tr, "surrogate": ms_sg, "scoring": ms_sc},
+                            "primaries_per_s_device": n_per / ((ms_tr + ms_sg + ms_sc) / 1000.0),
+                            "primaries_per_s_wall": n_per / wall}
+            stream_ms += ms_tr + ms_sg + ms_sc
+    tot = 3 * n_per
+    line = {"metric": "DNA-damage sweep primaries/s (1, 3, 10 keV; transport + surrogate + scoring)",
+            "value": tot / (stream_ms / 1000.0), "unit": "primaries/s", "n_gpus": 1, "steps": 1, "warmup": 0,
+            "ms_per_step": stream_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 transport / bf16-f32 surrogate", "data": "synthetic",
+            "config": {"workload": f"{n_per} primaries at each of 1, 3, 10 keV, batches of {B}, box +-15 um, "
+                                   "DNA 21 x 21 fibres, DSB window 10 bp", "training": train},
+            "yields": rows, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -491,12 +650,14 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--np", type=int, default=NP, help="primaries per GPU per step (4096 = the benchmark)")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", choices=["pipeline", "track", "mixed"], default="pipeline",
+    ap.add_argument("--workload", choices=["pipeline", "track", "mixed", "surrogate", "sweep"], default="pipeline",
                     help="pipeline = 4096 x 10 keV transport+IRT+scoring (the benchmark); track = one "
-                         "synthetic track through the IRT; mixed = 65,536 primaries of mixed energy")
+                         "synthetic track through the IRT; mixed = 65,536 primaries of mixed energy; "
+                         "surrogate = learned chemistry against the IRT; sweep = 1e6 primaries at 1, 3, 10 keV "
+                         "with surrogate chemistry and DNA scoring")
     args = ap.parse_args()
     if args.workload != "pipeline":
-        (run_track if args.workload == "track" else run_mixed)(args)
+        {"track": run_track, "mixed": run_mixed, "surrogate": run_surrogate, "sweep": run_sweep}[args.workload](args)
         return
     ws, rank, local = dist_init(args)
     try:

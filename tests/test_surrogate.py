@@ -101,3 +101,32 @@ def test_irt_curves_bit_exact(ctx):
     np.testing.assert_array_equal(cv, ref_["curves"][:n.value])
     # the curve at 1 us is the 7th checkpoint summed over tracks
     np.testing.assert_array_equal(cv[:, 15, :].sum(axis=0), ref_["tl"][6])
+
+
+@pytest.mark.gpu
+def test_trained_surrogate_against_irt(ctx):
+    """Train on the IRT's own curves at 3 and 10 keV, then judge a held-out
+    batch: the surrogate's G(1 us) against the IRT's, and its time against the
+    IRT's on the same tracks (what the network gains over the method alone)."""
+    from wgdna import surrogate as S
+    Xs, Gs = [], []
+    seed = 500
+    for E in (3000.0, 10000.0):
+        for _ in range(3):
+            X, G, _, _ = S.track_data(ctx, np.full(4096, E, np.float32), seed)
+            seed += 11
+            Xs.append(X); Gs.append(G)
+    losses = S.fit(ctx, np.concatenate(Xs), np.concatenate(Gs), schedule=((25, 2e-3), (10, 5e-4)), seed=3)
+    assert losses[-1] < 0.8 * losses[0]
+    L = _lib.lib()
+    Xh, Gh, Eh, ir = S.track_data(ctx, np.full(4096, 10000.0, np.float32), 424242)
+    gi, gp = S.batch_G(Gh, Eh), S.batch_G(S.predict(ctx, Xh), Eh)
+    rel = np.abs(gp[15] - gi[15]) / gi[15]
+    assert rel.max() < 0.05, (gi[15], gp[15])
+    # the whole-batch path on the device matches the host-side prediction
+    Gc = np.zeros(80)
+    ms = C.c_float()
+    _lib.check("chem", L.wgdna_surrogate_chemistry(ctx.h, _lib.ptr(Gc), C.byref(ms)))
+    if Xh.shape[0] == 4096:                                      # every track holds species
+        np.testing.assert_allclose(Gc.reshape(16, 5), gp, rtol=2e-3, atol=1e-4)
+    assert ms.value < ir.ms / 5, (ms.value, ir.ms)
