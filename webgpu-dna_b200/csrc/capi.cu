@@ -75,6 +75,7 @@ struct wgdna_ctx {
     size_t curves_cap = 0, curves_n = 0;
     size_t irt_slots = 0, irt_evslots = 0, irt_hov = 0, irt_pf_slots = 0;
     float4* d_pf = nullptr;
+    float4* d_rec = nullptr;
     float* d_tdel = nullptr;
     uint32_t irt_tracks = 0, irt_hcap = 0;
     double *d_px = nullptr, *d_py = nullptr, *d_pz = nullptr, *d_tb = nullptr;
@@ -212,7 +213,7 @@ extern "C" void wgdna_destroy(wgdna_ctx* c) {
                     c->d_red, c->d_err, c->d_fy, c->d_fz, c->d_rbb0, c->d_rbb1, c->d_hits, c->d_alive,
                     c->sc.info, c->sc.last_brk, c->sc.cnt0, c->sc.cnt1, c->sc.cs_in, c->sc.base, c->sc.u64,
                     c->sc.fib, c->d_px, c->d_py, c->d_pz, c->d_tb, c->d_sp, c->d_alive8, c->d_lst, c->d_lpos, c->d_evt, c->d_evab,
-                    c->d_hov_t, c->d_hov_ab, c->d_track, c->d_toff, c->d_irt_cnt, c->d_pf, c->d_tdel, c->d_curves, c->d_acc_tl, c->d_acc, c->d_maxpid};
+                    c->d_hov_t, c->d_hov_ab, c->d_track, c->d_toff, c->d_irt_cnt, c->d_pf, c->d_rec, c->d_tdel, c->d_curves, c->d_acc_tl, c->d_acc, c->d_maxpid};
     for (void* p : ptrs) if (p) cudaFree(p);
     for (auto& ev : c->ev) if (ev) cudaEventDestroy(ev);
     if (c->own) cudaStreamDestroy(c->own);
@@ -247,7 +248,7 @@ static IArgs make_iargs(wgdna_ctx* c, uint32_t nseg, uint64_t seed) {
     a.tn = c->d_track; a.th2 = c->d_track + T; a.ttiles = c->d_track + 2 * T; a.tev = c->d_track + 3 * T;
     a.tlc = c->d_track + 4 * T;
     a.toff = c->d_toff;
-    a.pf = c->d_pf; a.tdel = c->d_tdel;
+    a.pf = c->d_pf; a.rec = c->d_rec; a.tdel = c->d_tdel;
     a.hov_t = c->d_hov_t; a.hov_ab = c->d_hov_ab; a.hcap = c->irt_hcap;
     a.counters = c->d_irt_cnt;
     a.acc_tl = c->d_acc_tl; a.acc = c->d_acc; a.err = c->d_err;
@@ -390,6 +391,7 @@ static int irt_ensure(wgdna_ctx* c, uint32_t nseg, uint64_t rad_n, uint32_t cap)
     c->irt_hcap = (uint32_t)(hov / irt_warps(c->device));
     if (slots > c->irt_pf_slots) {
         TRY(dalloc(&c->d_pf, slots));
+        TRY(dalloc(&c->d_rec, 6 * slots));
         c->irt_pf_slots = slots;
     }
     if (nseg > c->irt_tracks) {

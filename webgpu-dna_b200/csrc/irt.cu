@@ -405,14 +405,18 @@ __global__ void __launch_bounds__(IB) k_irt_load(IArgs A) {
         __syncwarp();
         __threadfence_block();
         uint32_t cnt[6] = {0, 0, 0, 0, 0, 0};
+        float4* rec = A.rec + 6 * tb0;
         for (uint32_t c = 0; c < n; c += 32) {
             uint32_t k = c + lane;
             int spc = k < n ? sp[k] : -1;
+            float4 sh = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (k < n) { sh = pf[k]; sh.w = 0.0f; }               // shadow and birth time 0
             for (int q = 0; q < 6; ++q) {
                 unsigned m = __ballot_sync(FULL, spc == q);
                 if (spc == q) {
                     uint32_t at = cnt[q] + __popc(m & lt);
                     lst[q * cap + at] = (uint16_t)k;
+                    rec[q * cap + at] = sh;
                     lpos[k] = (uint16_t)at;
                 }
                 cnt[q] += __popc(m);
@@ -632,6 +636,9 @@ __global__ void __launch_bounds__(IB) k_irt_init(IArgs A) {
 __device__ __noinline__ u4 philox_pair(uint32_t id, uint32_t jj, uint32_t pid, uint32_t k0, uint32_t k1) {
     return philox(id, jj, pid, 5u, k0, k1);
 }
+__device__ __noinline__ u4 philox_pair_ang(uint32_t id, uint32_t jj, uint32_t pid, uint32_t k0, uint32_t k1) {
+    return philox(id, jj, pid, 5u | (1u << 4), k0, k1);
+}
 
 // the product being re-paired (uniform over the warp)
 struct ProdCtx {
@@ -718,7 +725,10 @@ __device__ __forceinline__ bool prod_batch(const IrtConst& C, const ProdCtx& P, 
 
 // 3) events (:566-660): sort the initial events, then pop in (t, i, j) order
 //    merged with a heap of product events; one warp per track
-__global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
+#ifndef WG_LOOP_MINB
+#define WG_LOOP_MINB 4
+#endif
+__global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
     __shared__ double s_tl[IB / 32][35];
     __shared__ double s_ht[IB / 32][HS];
     __shared__ uint32_t s_hab[IB / 32][HS];
@@ -736,8 +746,11 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
     for (int k = lane; k < 35; k += 32) s_tl[wl][k] = 0.0;
     int* lc = s_lc[wl];
     Heap H{s_ht[wl], s_hab[wl], A.hov_t + (size_t)gw * A.hcap, A.hov_ab + (size_t)gw * A.hcap};
-    unsigned long long rxn[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    unsigned long long n_reacted = 0, n_pairs = 0, n_events = 0, n_init = 0;
+    // per-warp tallies in shared memory (lane 0): reactions 0..8, reacted, events, initial events
+    __shared__ unsigned long long s_cnt[IB / 32][12];
+    unsigned long long* tally = s_cnt[wl];
+    for (int k = lane; k < 12; k += 32) tally[k] = 0;
+    unsigned long long n_pairs = 0;
     __syncwarp();
     for (;;) {
         uint32_t p = 0;
@@ -752,6 +765,7 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
         double* px = A.px + tb0; double* py = A.py + tb0; double* pz = A.pz + tb0; double* tb = A.tb + tb0;
         int8_t* sp = A.sp + tb0; uint8_t* alive = A.alive + tb0;
         uint16_t* lst = A.lst + 6 * tb0; uint16_t* lpos = A.lpos + tb0;
+        float4* rec = A.rec + 6 * tb0;
         double* ET = A.ev_t + ebase(A, p);
         uint32_t* EAB = A.ev_ab + ebase(A, p);
         const uint32_t nev = A.tev[p];
@@ -759,15 +773,11 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
         const float del = A.tdel[p];
         const float4 org = A.rad[A.seg_off[p]];
         const double ox = org.x, oy = org.y, oz = org.z;
-        // from here on the shadow's w holds the birth time (0 for the initial species)
-        for (uint32_t k = lane; k < n; k += 32) pf[k].w = 0.0f;
-        uint32_t cnt[6];
-        for (int q = 0; q < 6; ++q) cnt[q] = A.tlc[6 * p + q];
-        if (lane < 6) lc[lane] = (int)cnt[lane];
+        if (lane < 6) lc[lane] = (int)A.tlc[6 * p + lane];     // alive species of each kind
         uint32_t n2 = 1;
         while (n2 < nev) n2 <<= 1;
         if (nev > ecap(A, p)) { if (lane == 0) atomicOr(A.err, DERR_HEAP); continue; }
-        n_init += nev;
+        if (lane == 0) tally[11] += nev;
         __syncwarp();
         warp_sort(ET, EAB, nev, lane);
         uint32_t ip = 0, hn = 0;
@@ -789,16 +799,16 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
                     uint32_t ai = hi_ ? EAB[ip] : 0u, ah = hh ? H.ab(0) : 0u;
                     if (hi_ && (!hh || ev_less(ti, ai, th, ah))) { et = ti; eab = ai; ip++; }
                     else { et = th; eab = ah; heap_pop(H, hn); }
-                    n_events++;
+                    tally[10]++;
                     while (cp < 7 && et >= CP[cp]) {
-                        s_tl[wl][cp * 5 + 0] += cnt[0]; s_tl[wl][cp * 5 + 1] += cnt[1];
-                        s_tl[wl][cp * 5 + 2] += cnt[2]; s_tl[wl][cp * 5 + 3] += cnt[4];
+                        s_tl[wl][cp * 5 + 0] += lc[0]; s_tl[wl][cp * 5 + 1] += lc[1];
+                        s_tl[wl][cp * 5 + 2] += lc[2]; s_tl[wl][cp * 5 + 3] += lc[4];
                         s_tl[wl][cp * 5 + 4] += h2c;
                         cp++;
                     }
                     while (curve && c16 < 16 && et >= C.t16[c16]) {
                         float* c = curve + 5 * c16;
-                        c[0] = (float)cnt[0]; c[1] = (float)cnt[1]; c[2] = (float)cnt[2]; c[3] = (float)cnt[4];
+                        c[0] = (float)lc[0]; c[1] = (float)lc[1]; c[2] = (float)lc[2]; c[3] = (float)lc[4];
                         c[4] = (float)h2c;
                         c16++;
                     }
@@ -816,17 +826,17 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
                     if (ri >= 0) {
                         valid = 1;
                         alive[ei] = 0; alive[ej] = 0;
-                        cnt[si]--; cnt[sj]--;
                         for (int w2 = 0; w2 < 2; ++w2) {
                             int k = w2 == 0 ? ei : ej, q = w2 == 0 ? si : sj;
                             uint32_t at = lpos[k];
                             uint16_t last = lst[q * cap + lc[q] - 1];
                             lst[q * cap + at] = last;
+                            rec[q * cap + at] = rec[q * cap + lc[q] - 1];
                             lpos[last] = (uint16_t)at;
                             lc[q]--;
                         }
-                        n_reacted++;
-                        rxn[ri]++;
+                        tally[9]++;
+                        tally[ri]++;
                         if (ri == 3 || ri == 4 || ri == 6) h2c += 1;
                     }
                 }
@@ -858,9 +868,8 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
                 if (lane == 0) {
                     px[id] = nx; py[id] = ny; pz[id] = nz; tb[id] = et;
                     sp[id] = (int8_t)nsp; alive[id] = 1;
-                    pf[id] = make_float4(nsx, nsy, nsz, (float)et);
-                    cnt[nsp]++;
                     lst[nsp * cap + lc[nsp]] = (uint16_t)id;
+                    rec[nsp * cap + lc[nsp]] = make_float4(nsx, nsy, nsz, (float)et);
                     lpos[id] = (uint16_t)lc[nsp];
                     lc[nsp]++;
                 }
@@ -882,6 +891,7 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
                     const float Djf2 = (float)(2.0 * C.D[s2]);
                     const float fs = C.fs[r2i], fsc = C.fsc[r2i], fadd = C.fadd[r2i];
                     const uint16_t* L2 = lst + s2 * cap;
+                    const float4* R2 = rec + s2 * cap;
                     // PU chunks of 32 partners at a time: independent loads and Philox blocks
                     for (uint32_t c0 = 0; c0 < len; c0 += 32 * PU) {
                         uint32_t jv[PU];
@@ -893,8 +903,10 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
                         }
                         float4 qv[PU];
 #pragma unroll
-                        for (int u = 0; u < PU; ++u)
-                            if (jv[u] != 0xffffu) qv[u] = pf[jv[u]];
+                        for (int u = 0; u < PU; ++u) {
+                            const uint32_t li = c0 + 32u * u + lane;
+                            if (li < len) qv[u] = R2[li];
+                        }
 #pragma unroll
                         for (int u = 0; u < PU; ++u) {
                             const uint32_t jj = jv[u];
@@ -910,15 +922,33 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
                                 const float rhi = (fmaxf(fs, __fdividef(fsc, uf)) + fadd) * 1.00002f + 1e-6f;
                                 // upper bound of dt = et - t_birth from the f32 birth time (error < dtm)
                                 const float dth = etf - q.w + dtm;
-                                float reach = 0.0f;
+                                float reach = 0.0f, l0 = 0.0f, l1 = 0.0f, l2 = 0.0f, Bf = 0.0f;
                                 if (dth > 0.0f) {
-                                    const float l0 = -2.0f * __logf((float)u01d32(q0.x));
-                                    const float l1 = -2.0f * __logf((float)u01d32(q0.y));
-                                    const float l2 = -2.0f * __logf((float)u01d32(q0.z));
-                                    const float Bf = sqrtf((l0 + l1 + l2) * 1.0001f);
+                                    l0 = -2.0f * __logf((float)u01d32(q0.x));
+                                    l1 = -2.0f * __logf((float)u01d32(q0.y));
+                                    l2 = -2.0f * __logf((float)u01d32(q0.z));
+                                    Bf = sqrtf((l0 + l1 + l2) * 1.0001f);
                                     reach = sqrtf(Djf2 * dth) * 1.00001f * (Bf + 1e-4f);
                                 }
                                 mv[u] = !(dlo - reach > rhi);
+                                if (mv[u] && dth > 0.0f) {
+                                    // second stage: the partner displaced by the same Box-Muller draws in
+                                    // f32.  Per axis |g_f - g| <= 2e-3 + 2e-5 |g| (sqrt of the log near 0,
+                                    // fast log and cos, 2 ulp each), sigma within [sl, sh].
+                                    const u4 q1 = philox_pair_ang(id, jj, pid, A.k0, A.k1);
+                                    const float dtl = fmaxf(etf - q.w - dtm, 0.0f);
+                                    const float sh = sqrtf(Djf2 * dth) * 1.00001f, sl = sqrtf(Djf2 * dtl) * 0.99999f;
+                                    const float sm = 0.5f * (sh + sl), Bm = Bf + 1e-4f;
+                                    // cos(2 pi u) = -cos(2 pi (u - 1/2)): the argument stays in [-pi, pi]
+                                    const float g0 = -sqrtf(l0) * __cosf(6.2831853f * ((float)u01d32(q1.x) - 0.5f));
+                                    const float g1 = -sqrtf(l1) * __cosf(6.2831853f * ((float)u01d32(q1.y) - 0.5f));
+                                    const float g2 = -sqrtf(l2) * __cosf(6.2831853f * ((float)u01d32(q1.z) - 0.5f));
+                                    const float fx = ex - g0 * sm, fy = ey - g1 * sm, fz = ez - g2 * sm;
+                                    const float d2 = sqrtf(fmaf(fz, fz, fmaf(fy, fy, fx * fx)));
+                                    const float eg = 2e-3f + 2e-5f * Bm;
+                                    const float err = 1.7320508f * (sh * eg + 0.5f * (Bm + eg) * (sh - sl)) + del;
+                                    mv[u] = !((d2 - err) * 0.99999f > rhi);
+                                }
                             }
                         }
 #pragma unroll
@@ -950,33 +980,29 @@ __global__ void __launch_bounds__(IB) k_irt_loop(IArgs A) {
         if (lane == 0) {
             if (heap_over) atomicOr(A.err, DERR_HEAP);
             while (cp < 7) {
-                s_tl[wl][cp * 5 + 0] += cnt[0]; s_tl[wl][cp * 5 + 1] += cnt[1];
-                s_tl[wl][cp * 5 + 2] += cnt[2]; s_tl[wl][cp * 5 + 3] += cnt[4];
+                s_tl[wl][cp * 5 + 0] += lc[0]; s_tl[wl][cp * 5 + 1] += lc[1];
+                s_tl[wl][cp * 5 + 2] += lc[2]; s_tl[wl][cp * 5 + 3] += lc[4];
                 s_tl[wl][cp * 5 + 4] += h2c;
                 cp++;
             }
             while (curve && c16 < 16) {
                 float* c = curve + 5 * c16;
-                c[0] = (float)cnt[0]; c[1] = (float)cnt[1]; c[2] = (float)cnt[2]; c[3] = (float)cnt[4];
+                c[0] = (float)lc[0]; c[1] = (float)lc[1]; c[2] = (float)lc[2]; c[3] = (float)lc[4];
                 c[4] = (float)h2c;
                 c16++;
             }
         }
         __syncwarp();
     }
-    for (int k = 0; k < 9; ++k) {
-        unsigned long long v = rxn[k];
-        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-        if (lane == 0 && v) atomicAdd(&A.acc[k], v);
-    }
-    if (lane == 0 && n_init) atomicAdd(&A.acc[14], n_init);
-    unsigned long long vals[3] = {n_reacted, n_pairs, n_events};
-    for (int k = 0; k < 3; ++k) {
-        unsigned long long v = vals[k];
-        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-        if (lane == 0 && v) atomicAdd(&A.acc[9 + k], v);
-    }
+    for (int o = 16; o; o >>= 1) n_pairs += __shfl_xor_sync(FULL, n_pairs, o);
     __syncwarp();
+    if (lane == 0) {
+        for (int k = 0; k < 9; ++k) if (tally[k]) atomicAdd(&A.acc[k], tally[k]);
+        if (tally[9]) atomicAdd(&A.acc[9], tally[9]);
+        if (n_pairs) atomicAdd(&A.acc[10], n_pairs);
+        if (tally[10]) atomicAdd(&A.acc[11], tally[10]);
+        if (tally[11]) atomicAdd(&A.acc[14], tally[11]);
+    }
     for (int k = lane; k < 35; k += 32)
         if (s_tl[wl][k] != 0.0) atomicAdd(&A.acc_tl[k], s_tl[wl][k]);
 }

@@ -29,8 +29,8 @@ struct IArgs {
     uint8_t* alive;
     uint16_t* lst;                       // 6 lists per track: alive particles of each species
     uint16_t* lpos;                      // position of a particle in its list
-    float4* pf;                          // f32 shadow (x, y, z relative to the track origin; w: species bits,
-                                         // in the event kernel the birth time)
+    float4* rec;                         // the lists' records: f32 shadow x, y, z and birth time
+    float4* pf;                          // f32 shadow (x, y, z relative to the track origin; w: species bits)
     float* tdel;                         // per track: bound on the shadow's distance error (nm)
     double* ev_t;                        // initial events of each track
     uint32_t* ev_ab;                     // packed (a << 16) | b
