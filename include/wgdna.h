@@ -169,6 +169,22 @@ int wgdna_cluster_dsb(wgdna_ctx *ctx, const uint8_t *hits, wgdna_dsb_result *out
  * (app.ts:182-185 with the worker backend, where indirect scoring is skipped). */
 int wgdna_score(wgdna_ctx *ctx, uint32_t lcg_state, wgdna_ssb_result *ssb, wgdna_dsb_result *dsb);
 
+/* Dose-grid reductions and dose-based scoring.  dose: a host vc^3 grid, or
+ * NULL for the grid of the last wgdna_transport on the device. */
+/* sumDoseEV (src/scoring/dose.ts:13-17): the grid's sum / 100. */
+int wgdna_dose_sum(wgdna_ctx *ctx, const uint32_t *dose, double *eV);
+/* The projection sums of renderDoseProjection (dose.ts:61-85): axis 0 sums over
+ * z into proj[y][x], axis 1 over x into proj[z][y]; vc^2 floats. */
+int wgdna_dose_projection(wgdna_ctx *ctx, const uint32_t *dose, int axis, float *proj);
+/* scoreDirectSSB (ssb-dsb.ts:227-283): expected direct SSBs from the voxel dose
+ * at the backbone sites of the context's DNA target; lambda (2 * n_bp floats,
+ * may be NULL) receives the per-site expectations and stays on the device. */
+int wgdna_score_voxel_ssb(wgdna_ctx *ctx, const uint32_t *dose, double box_nm, float *lambda,
+                          double *direct_expected);
+/* expectedDSBLocal (ssb-dsb.ts:285-334) on lambda (NULL: the last
+ * wgdna_score_voxel_ssb) and indirect hit bytes (NULL: none). */
+int wgdna_expected_dsb_local(wgdna_ctx *ctx, const float *lambda, const uint8_t *hits, double *dsb_expected);
+
 /* ---------------------------------------------------------------- surrogate */
 /* Learned chemistry (no reference counterpart): an MLP 64 -> 128 -> 128 ->
  * 128 -> 80 with GELU, bf16 weights and f32 accumulation on the tensor cores,

@@ -89,6 +89,13 @@ def lib():
                                          C.c_uint32, P(C.c_uint8), P(SsbOut)]
         L.orc_cluster_dsb.argtypes = [P(Dna), P(C.c_uint8), P(C.c_uint64), P(C.c_double),
                                       P(C.c_uint64), P(C.c_uint64)]
+        L.orc_voxel_ssb.argtypes = [P(Dna), P(C.c_uint32), C.c_uint32, C.c_double, P(C.c_float)]
+        L.orc_voxel_ssb.restype = C.c_double
+        L.orc_expected_dsb_local.argtypes = [P(Dna), P(C.c_float), P(C.c_uint8)]
+        L.orc_expected_dsb_local.restype = C.c_double
+        L.orc_dose_sum_ev.argtypes = [P(C.c_uint32), C.c_uint64]
+        L.orc_dose_sum_ev.restype = C.c_double
+        L.orc_dose_projection.argtypes = [P(C.c_uint32), C.c_uint32, C.c_int, P(C.c_float)]
         rc = L.orc_load_tables(BLOB.encode())
         if rc != 0:
             raise RuntimeError(f"oracle: cannot load tables {BLOB} (rc={rc})")
@@ -221,3 +228,30 @@ def cluster_dsb(dna, hits):
     lib().orc_cluster_dsb(C.byref(dna._d), _fp(hits, C.c_uint8), C.byref(dsb), C.byref(de),
                           C.byref(s0), C.byref(s1))
     return dict(dsb=dsb.value, dsb_expected=de.value, ssb0=s0.value, ssb1=s1.value)
+
+
+def voxel_ssb(dna, dose, box_nm=15000.0, vc=128):
+    """scoreDirectSSB (ssb-dsb.ts:227-283): (direct_expected, lambda)."""
+    dose = np.ascontiguousarray(dose, dtype=np.uint32)
+    lam = np.zeros(2 * dna.n_bp, np.float32)
+    e = lib().orc_voxel_ssb(C.byref(dna._d), _fp(dose, C.c_uint32), vc, box_nm, _fp(lam))
+    return e, lam
+
+
+def expected_dsb_local(dna, lam, hits=None):
+    """expectedDSBLocal (ssb-dsb.ts:285-334)."""
+    lam = np.ascontiguousarray(lam, dtype=np.float32)
+    h = None if hits is None else _fp(np.ascontiguousarray(hits, dtype=np.uint8), C.c_uint8)
+    return lib().orc_expected_dsb_local(C.byref(dna._d), _fp(lam), h)
+
+
+def dose_sum_ev(dose):
+    dose = np.ascontiguousarray(dose, dtype=np.uint32)
+    return lib().orc_dose_sum_ev(_fp(dose, C.c_uint32), dose.size)
+
+
+def dose_projection(dose, axis, vc=128):
+    dose = np.ascontiguousarray(dose, dtype=np.uint32)
+    out = np.zeros(vc * vc, np.float32)
+    lib().orc_dose_projection(_fp(dose, C.c_uint32), vc, axis, _fp(out))
+    return out.reshape(vc, vc)

@@ -107,6 +107,12 @@ int orc_score_indirect(const orc_dna *d, const float *pos, const uint32_t *alive
 int orc_cluster_dsb(const orc_dna *d, const uint8_t *hits, uint64_t *dsb, double *dsb_expected,
                     uint64_t *ssb0, uint64_t *ssb1);
 
+/* dose-grid scoring (ssb-dsb.ts:227-334) and dose reductions (dose.ts:13-85) */
+double orc_voxel_ssb(const orc_dna *d, const uint32_t *dose, uint32_t vc, double box_nm, float *lambda);
+double orc_expected_dsb_local(const orc_dna *d, const float *lambda, const uint8_t *hits);
+double orc_dose_sum_ev(const uint32_t *dose, uint64_t n);
+void orc_dose_projection(const uint32_t *dose, uint32_t vc, int axis, float *proj);
+
 #ifdef __cplusplus
 }
 #endif

@@ -181,3 +181,99 @@ int orc_cluster_dsb(const orc_dna *d, const uint8_t *hits, uint64_t *dsb, double
     *dsb = di; *dsb_expected = de; *ssb0 = t0; *ssb1 = t1;
     return 0;
 }
+
+/* ---- dose-grid scoring (src/scoring/ssb-dsb.ts:227-334) and reductions
+ * (src/scoring/dose.ts:13-85), JS number semantics: f64 arithmetic, f32 where
+ * the reference stores into a Float32Array. */
+
+/* scoreDirectSSB: expected direct SSBs from the voxel dose at each backbone
+ * site.  lambda (2 * n_bp floats) receives the per-site expectations; strand
+ * 1 divides the dose by 10 where strand 0 divides by 100, as the reference
+ * does (ssb-dsb.ts:273-276). */
+double orc_voxel_ssb(const orc_dna *d, const uint32_t *dose, uint32_t vc, double box_nm, float *lambda) {
+    const double vox_nm = (2 * box_nm) / vc;
+    const double vox_vol = vox_nm * vox_nm * vox_nm;
+    const double half = box_nm;
+    const double inv_vox = 1 / vox_nm;
+    const double r = 0.29;                                       /* SSB_R_DAMAGE_NM */
+    const double bb_vol_per_bp = (4.0 / 3) * M_PI * r * r * r;
+    const double K = ((bb_vol_per_bp / vox_vol) * 0.15) / 22;   /* SSB_P_DIRECT, E_mean_ion */
+    const uint64_t n = d->n_bp;
+    double direct = 0;
+    memset(lambda, 0, 2 * n * sizeof(float));
+    for (uint32_t fi = 0; fi < d->n_fibers; ++fi) {
+        const double fy = d->fy[fi], fz = d->fz[fi];
+        const uint64_t base = (uint64_t)fi * d->n_bp_per;
+        for (uint32_t b = 0; b < d->n_bp_per; ++b) {
+            const double bx = d->x0 + b * d->rise;
+            const double vx = floor((bx + half) * inv_vox);
+            if (vx < 0 || vx >= vc) continue;
+            const double y0 = fy + d->rbb0[2 * b], z0 = fz + d->rbb0[2 * b + 1];
+            const double y1 = fy + d->rbb1[2 * b], z1 = fz + d->rbb1[2 * b + 1];
+            const double vy0 = floor((y0 + half) * inv_vox), vz0 = floor((z0 + half) * inv_vox);
+            const double vy1 = floor((y1 + half) * inv_vox), vz1 = floor((z1 + half) * inv_vox);
+            if (vy0 >= 0 && vy0 < vc && vz0 >= 0 && vz0 < vc) {
+                const double dd = dose[(uint64_t)((vz0 * vc + vy0) * vc + vx)] / 100.0;
+                const double l = dd * K;
+                lambda[base + b] = (float)l;
+                direct += l;
+            }
+            if (vy1 >= 0 && vy1 < vc && vz1 >= 0 && vz1 < vc) {
+                const double dd = dose[(uint64_t)((vz1 * vc + vy1) * vc + vx)] / 10.0;
+                const double l = dd * K;
+                lambda[n + base + b] = (float)l;
+                direct += l;
+            }
+        }
+    }
+    return direct;
+}
+
+/* expectedDSBLocal: per fibre, strand-0 density times the strand-1 density
+ * summed over +-DSB_WINDOW_BP, densities = lambda + indirect hit indicator. */
+double orc_expected_dsb_local(const orc_dna *d, const float *lambda, const uint8_t *hits) {
+    const int64_t W = 10, n_per = d->n_bp_per;
+    const uint64_t n = d->n_bp;
+    float *s0 = (float *)malloc(n_per * sizeof(float)), *s1 = (float *)malloc(n_per * sizeof(float));
+    double e = 0;
+    for (uint32_t fi = 0; fi < d->n_fibers; ++fi) {
+        const uint64_t base = (uint64_t)fi * n_per;
+        double sum0 = 0, sum1 = 0;
+        for (int64_t b = 0; b < n_per; ++b) {
+            const double v0 = (double)lambda[base + b] + ((hits && hits[base + b] == 1) ? 1 : 0);
+            const double v1 = (double)lambda[n + base + b] + ((hits && hits[n + base + b] == 1) ? 1 : 0);
+            s0[b] = (float)v0; s1[b] = (float)v1;
+            sum0 += v0; sum1 += v1;
+        }
+        if (sum0 == 0 || sum1 == 0) continue;
+        double win = 0;
+        for (int64_t b = 0; b <= (W < n_per - 1 ? W : n_per - 1); ++b) win += s1[b];
+        for (int64_t b = 0; b < n_per; ++b) {
+            e += s0[b] * win;
+            const int64_t lo = b - W, hi = b + 1 + W;
+            if (hi < n_per) win += s1[hi];
+            if (lo >= 0) win -= s1[lo];
+        }
+    }
+    free(s0); free(s1);
+    return e;
+}
+
+/* sumDoseEV (dose.ts:13-17): the exact integer sum / 100 */
+double orc_dose_sum_ev(const uint32_t *dose, uint64_t n) {
+    uint64_t s = 0;
+    for (uint64_t i = 0; i < n; ++i) s += dose[i];
+    return (double)s / 100.0;
+}
+
+/* projection sums of renderDoseProjection (dose.ts:61-85): axis 0 sums over z
+ * into [y][x], axis 1 over x into [z][y]; stored as float like the reference */
+void orc_dose_projection(const uint32_t *dose, uint32_t vc, int axis, float *proj) {
+    for (uint32_t a = 0; a < vc; ++a)
+        for (uint32_t b = 0; b < vc; ++b) {
+            uint64_t s = 0;
+            for (uint32_t c = 0; c < vc; ++c)
+                s += axis == 0 ? dose[((uint64_t)c * vc + a) * vc + b] : dose[((uint64_t)a * vc + b) * vc + c];
+            proj[(uint64_t)a * vc + b] = (float)(double)s;
+        }
+}

@@ -8,6 +8,7 @@
 
 #include "common.cuh"
 
+#include "dose.cuh"
 #include "irt.cuh"
 #include "scoring.cuh"
 #include "surrogate_api.cuh"
@@ -60,6 +61,12 @@ struct wgdna_ctx {
     float last_E = 0.0f;
     bool last_has_eprim = false;
     wg::SgState* sg = nullptr;           // surrogate chemistry (surrogate_api.cu)
+    // dose-based scoring: an uploaded grid, per-site lambda, uploaded hits, f64 / u64 results
+    uint32_t* d_dose_in = nullptr;
+    float* d_lambda = nullptr;
+    uint8_t* d_hits_in = nullptr;
+    double* d_dres = nullptr;
+    bool have_lambda = false;
     unsigned long long last_rad_n = 0;
     // DNA target + scoring
     wgdna_dna_info dna{};
@@ -213,7 +220,8 @@ extern "C" void wgdna_destroy(wgdna_ctx* c) {
                     c->d_red, c->d_err, c->d_fy, c->d_fz, c->d_rbb0, c->d_rbb1, c->d_hits, c->d_alive,
                     c->sc.info, c->sc.last_brk, c->sc.cnt0, c->sc.cnt1, c->sc.cs_in, c->sc.base, c->sc.u64,
                     c->sc.fib, c->d_px, c->d_py, c->d_pz, c->d_tb, c->d_sp, c->d_alive8, c->d_lst, c->d_lpos, c->d_evt, c->d_evab,
-                    c->d_hov_t, c->d_hov_ab, c->d_track, c->d_toff, c->d_irt_cnt, c->d_pf, c->d_rec, c->d_tdel, c->d_curves, c->d_acc_tl, c->d_acc, c->d_maxpid};
+                    c->d_hov_t, c->d_hov_ab, c->d_track, c->d_toff, c->d_irt_cnt, c->d_pf, c->d_rec, c->d_tdel, c->d_curves, c->d_acc_tl, c->d_acc, c->d_maxpid,
+                    c->d_dose_in, c->d_lambda, c->d_hits_in, c->d_dres};
     for (void* p : ptrs) if (p) cudaFree(p);
     for (auto& ev : c->ev) if (ev) cudaEventDestroy(ev);
     if (c->own) cudaStreamDestroy(c->own);
@@ -784,5 +792,96 @@ extern "C" int wgdna_reaction_table(double out[9][6]) {
         out[r][0] = C.sigma[r]; out[r][1] = C.sigma_eff[r]; out[r][2] = C.rc[r];
         out[r][3] = C.kdif[r]; out[r][4] = C.kact[r]; out[r][5] = C.prob[r];
     }
+    return WGDNA_OK;
+}
+
+// ------------------------------------------------------------------ dose-grid scoring
+// the grid to use: a host grid (uploaded) or the last transport's
+static int dose_source(wgdna_ctx* c, const uint32_t* dose, const uint32_t** out) {
+    const size_t nv = (size_t)c->cfg.vc * c->cfg.vc * c->cfg.vc;
+    if (dose) {
+        if (!c->d_dose_in) TRY(dalloc(&c->d_dose_in, nv));
+        WG_CUDA_OK(cudaMemcpyAsync(c->d_dose_in, dose, nv * 4, cudaMemcpyHostToDevice, c->stream));
+        *out = c->d_dose_in;
+        return WGDNA_OK;
+    }
+    if (!c->have_transport) { wg_set_error("no dose grid: pass one or run wgdna_transport first"); return WGDNA_ERR_STATE; }
+    *out = c->d_dose;
+    return WGDNA_OK;
+}
+
+static wg::DoseDna dose_dna(wgdna_ctx* c) {
+    wg::DoseDna d;
+    d.fy = c->d_fy; d.fz = c->d_fz; d.rbb0 = c->d_rbb0; d.rbb1 = c->d_rbb1;
+    d.n_fibers = c->dna.n_fibers; d.n_bp_per = c->dna.n_bp_per; d.x0 = c->dna.x0; d.rise = c->dna.rise;
+    return d;
+}
+
+extern "C" int wgdna_dose_sum(wgdna_ctx* c, const uint32_t* dose, double* eV) {
+    if (!c || !eV) { wg_set_error("wgdna_dose_sum: NULL argument"); return WGDNA_ERR_ARG; }
+    WG_CUDA_OK(cudaSetDevice(c->device));
+    const uint32_t* g = nullptr;
+    TRY(dose_source(c, dose, &g));
+    if (!c->d_dres) TRY(dalloc(&c->d_dres, 4));
+    const size_t nv = (size_t)c->cfg.vc * c->cfg.vc * c->cfg.vc;
+    WG_CUDA_OK(launch_dose_sum(g, nv, reinterpret_cast<unsigned long long*>(c->d_dres), c->stream));
+    unsigned long long u = 0;
+    WG_CUDA_OK(cudaMemcpyAsync(&u, c->d_dres, 8, cudaMemcpyDeviceToHost, c->stream));
+    WG_CUDA_OK(cudaStreamSynchronize(c->stream));
+    *eV = (double)u / 100.0;
+    return WGDNA_OK;
+}
+
+extern "C" int wgdna_dose_projection(wgdna_ctx* c, const uint32_t* dose, int axis, float* proj) {
+    if (!c || !proj || (axis != 0 && axis != 1)) { wg_set_error("wgdna_dose_projection: bad argument"); return WGDNA_ERR_ARG; }
+    WG_CUDA_OK(cudaSetDevice(c->device));
+    const uint32_t* g = nullptr;
+    TRY(dose_source(c, dose, &g));
+    const uint32_t vc = c->cfg.vc;
+    float* d = nullptr;
+    TRY(dalloc(&d, (size_t)vc * vc));
+    WG_CUDA_OK(launch_dose_projection(g, vc, axis, d, c->stream));
+    WG_CUDA_OK(cudaMemcpyAsync(proj, d, (size_t)vc * vc * 4, cudaMemcpyDeviceToHost, c->stream));
+    WG_CUDA_OK(cudaStreamSynchronize(c->stream));
+    cudaFree(d);
+    return WGDNA_OK;
+}
+
+extern "C" int wgdna_score_voxel_ssb(wgdna_ctx* c, const uint32_t* dose, double box_nm, float* lambda,
+                                     double* direct_expected) {
+    if (!c) { wg_set_error("wgdna_score_voxel_ssb: NULL context"); return WGDNA_ERR_ARG; }
+    WG_CUDA_OK(cudaSetDevice(c->device));
+    const uint32_t* g = nullptr;
+    TRY(dose_source(c, dose, &g));
+    const size_t nl = 2 * (size_t)c->dna.n_bp;
+    if (!c->d_lambda) TRY(dalloc(&c->d_lambda, nl));
+    if (!c->d_dres) TRY(dalloc(&c->d_dres, 4));
+    WG_CUDA_OK(launch_voxel_ssb(dose_dna(c), g, c->cfg.vc, box_nm, c->d_lambda, c->d_dres, c->stream));
+    double e = 0;
+    WG_CUDA_OK(cudaMemcpyAsync(&e, c->d_dres, 8, cudaMemcpyDeviceToHost, c->stream));
+    if (lambda) WG_CUDA_OK(cudaMemcpyAsync(lambda, c->d_lambda, nl * 4, cudaMemcpyDeviceToHost, c->stream));
+    WG_CUDA_OK(cudaStreamSynchronize(c->stream));
+    c->have_lambda = true;
+    if (direct_expected) *direct_expected = e;
+    return WGDNA_OK;
+}
+
+extern "C" int wgdna_expected_dsb_local(wgdna_ctx* c, const float* lambda, const uint8_t* hits, double* dsb_expected) {
+    if (!c || !dsb_expected) { wg_set_error("wgdna_expected_dsb_local: NULL argument"); return WGDNA_ERR_ARG; }
+    WG_CUDA_OK(cudaSetDevice(c->device));
+    const size_t nl = 2 * (size_t)c->dna.n_bp;
+    if (!c->d_lambda) TRY(dalloc(&c->d_lambda, nl));
+    if (lambda) WG_CUDA_OK(cudaMemcpyAsync(c->d_lambda, lambda, nl * 4, cudaMemcpyHostToDevice, c->stream));
+    else if (!c->have_lambda) { wg_set_error("wgdna_expected_dsb_local: no lambda (run wgdna_score_voxel_ssb or pass one)"); return WGDNA_ERR_STATE; }
+    const uint8_t* dh = nullptr;
+    if (hits) {
+        if (!c->d_hits_in) TRY(dalloc(&c->d_hits_in, nl));
+        WG_CUDA_OK(cudaMemcpyAsync(c->d_hits_in, hits, nl, cudaMemcpyHostToDevice, c->stream));
+        dh = c->d_hits_in;
+    }
+    if (!c->d_dres) TRY(dalloc(&c->d_dres, 4));
+    WG_CUDA_OK(launch_expected_dsb(dose_dna(c), c->d_lambda, dh, c->d_dres, c->stream));
+    WG_CUDA_OK(cudaMemcpyAsync(dsb_expected, c->d_dres, 8, cudaMemcpyDeviceToHost, c->stream));
+    WG_CUDA_OK(cudaStreamSynchronize(c->stream));
     return WGDNA_OK;
 }

@@ -24,7 +24,8 @@ EXPORTS = ["wgdna_default_cfg", "wgdna_create", "wgdna_destroy", "wgdna_last_err
            "wgdna_score_direct_noalloc", "wgdna_reaction_table", "wgdna_irt_record_curves", "wgdna_irt_curves",
            "wgdna_track_descriptors", "wgdna_surrogate_init", "wgdna_surrogate_params", "wgdna_surrogate_norm",
            "wgdna_surrogate_load", "wgdna_surrogate_train", "wgdna_surrogate_grad", "wgdna_surrogate_predict",
-           "wgdna_surrogate_chemistry"]
+           "wgdna_surrogate_chemistry", "wgdna_dose_sum", "wgdna_dose_projection", "wgdna_score_voxel_ssb",
+           "wgdna_expected_dsb_local"]
 SG_IN, SG_OUT, SG_NPARAM = 64, 80, 51664
 
 
@@ -127,6 +128,10 @@ def lib():
         "wgdna_surrogate_grad": (C.c_int, [vp, C.c_uint64, vp, P(C.c_double)]),
         "wgdna_surrogate_predict": (C.c_int, [vp, vp, C.c_uint64, vp]),
         "wgdna_surrogate_chemistry": (C.c_int, [vp, vp, P(C.c_float)]),
+        "wgdna_dose_sum": (C.c_int, [vp, vp, P(C.c_double)]),
+        "wgdna_dose_projection": (C.c_int, [vp, vp, C.c_int, vp]),
+        "wgdna_score_voxel_ssb": (C.c_int, [vp, vp, C.c_double, vp, P(C.c_double)]),
+        "wgdna_expected_dsb_local": (C.c_int, [vp, vp, vp, P(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

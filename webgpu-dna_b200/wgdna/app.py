@@ -125,5 +125,48 @@ def results_json(rows, n_primaries):
     return None
 
 
+def classify(ratio):
+    """classify (src/ui/table.ts:21-25): 'ok' within 10 %, 'meh' within 2x, else 'bad'."""
+    if 0.9 <= ratio <= 1.1:
+        return "ok"
+    if 0.5 <= ratio <= 2.0:
+        return "meh"
+    return "bad"
+
+
+def results_table(rows):
+    """The cells of the results table, one dict per energy, in the order of
+    appendResultRow (src/ui/table.ts:38-73)."""
+    out = []
+    for row in rows:
+        r, est = row["result"], row["ref"]
+        d = row["damage"] or {"ssb_dir": 0, "ssb_ind": 0, "dsb": 0, "dsb_per_gy_gbp": 0}
+        csda_ratio = r["mean_total"] / est["csda"]
+        sp_ratio = r["mean_sp"] / est["sp"]
+        out.append({
+            "E_eV": r["E"], "n_therm": r["n_therm"], "n_esc": r["n_esc"],
+            "csda_nm": r["mean_total"], "estar_csda_nm": est["csda"], "csda_ratio": csda_ratio,
+            "csda_class": classify(csda_ratio),
+            "prod_path_nm": r["mean_prod"], "sp_eV_per_nm": r["mean_sp"], "estar_sp": est["sp"],
+            "sp_ratio": sp_ratio, "sp_class": classify(sp_ratio),
+            "ions_per_primary": r["mean_ions"], "sec_per_primary": r["sec_per_pri"], "sec_dropped": r["sec_dropped"],
+            "e_conservation": r["cons_ratio"], "e_conservation_class": classify(r["cons_ratio"]),
+            "G_OH_init": r["G_OH"], "G_eaq_init": r["G_eaq"], "G_H_init": r["G_H"],
+            "SSB_dir": d["ssb_dir"], "SSB_ind": d["ssb_ind"], "DSB": d["dsb"], "DSB_per_Gy_Gbp": d["dsb_per_gy_gbp"],
+            "dt_ms": r["dt"],
+        })
+    return out
+
+
+def write_results(rows, n_primaries, path):
+    """The sweep's results as JSON: every energy's table row plus the
+    validation/webgpu-results.json shape of the 10 keV row."""
+    import json
+    doc = {"rows": results_table(rows), "tenKeV": results_json(rows, n_primaries)}
+    with open(path, "w") as f:
+        json.dump(doc, f, indent=1, default=float)
+    return doc
+
+
 runValidation = run_validation
 ensurePipelines = ensure_pipelines
