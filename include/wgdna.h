@@ -130,6 +130,24 @@ int wgdna_irt_curves(wgdna_ctx *ctx, float *out, uint64_t cap_tracks, uint64_t *
  * the worker reports sigma and rc in its rxn_info (irt-worker.js:690-694). */
 int wgdna_reaction_table(double out[9][6]);
 
+/* The reference's 'gpu' chemistry backend (src/shaders/chemistry.wgsl,
+ * src/chemistry/schedule.ts:33-247): diffusion in fixed steps, a spatial hash
+ * of 1.5 nm cells, contact reactions with compare-and-swap claims (so results
+ * vary with thread timing, as in the reference), on the first
+ * min(rad_n, 8,000,000) entries of rad (NULL: the last transport's rad_buf).
+ * Checkpoints: t = 0 and 1 ps, 10 ps, 100 ps, 1 ns, 10 ns, 100 ns, 1 us.
+ * pos (x, y, z, kind) and alive of the radicals when cap >= chem_n, for
+ * scoreIndirectSSB (wgdna_score_indirect); either may be NULL. */
+typedef struct {
+    uint32_t counts[8][5];      /* alive OH, eaq, H; H2O2 and H2 made */
+    double G[8][5];             /* per 100 eV of n_therm * E_eV * chem_n / rad_n */
+    uint64_t chem_n;
+    double deposited_eV;
+    float ms;
+} wgdna_chem_grid_result;
+int wgdna_chem_grid(wgdna_ctx *ctx, const float *rad, uint64_t rad_n, uint32_t n_therm, double E_eV,
+                    uint64_t seed, wgdna_chem_grid_result *out, float *pos, uint32_t *alive, uint64_t cap);
+
 /* ---------------------------------------------------------------- scoring */
 typedef struct {
     uint32_t grid_N, n_bp_per, n_fibers, n_bp;

@@ -96,6 +96,8 @@ def lib():
         L.orc_dose_sum_ev.argtypes = [P(C.c_uint32), C.c_uint64]
         L.orc_dose_sum_ev.restype = C.c_double
         L.orc_dose_projection.argtypes = [P(C.c_uint32), C.c_uint32, C.c_int, P(C.c_float)]
+        L.orc_chem_grid.argtypes = [P(C.c_float), C.c_uint32, C.c_uint64, P(C.c_float), P(C.c_uint32),
+                                    P(C.c_uint32)]
         rc = L.orc_load_tables(BLOB.encode())
         if rc != 0:
             raise RuntimeError(f"oracle: cannot load tables {BLOB} (rc={rc})")
@@ -255,3 +257,16 @@ def dose_projection(dose, axis, vc=128):
     out = np.zeros(vc * vc, np.float32)
     lib().orc_dose_projection(_fp(dose, C.c_uint32), vc, axis, _fp(out))
     return out.reshape(vc, vc)
+
+
+def chem_grid(rad, seed=0, n=None):
+    """Grid-hash chemistry on the first n entries of rad: (counts 8 x 5, pos, alive)."""
+    rad = np.ascontiguousarray(rad, dtype=np.float32).reshape(-1, 4)
+    n = rad.shape[0] if n is None else min(n, rad.shape[0])
+    pos = np.zeros((n, 4), np.float32)
+    alive = np.zeros(n, np.uint32)
+    counts = np.zeros((8, 5), np.uint32)
+    rc = lib().orc_chem_grid(_fp(rad), n, seed, _fp(pos), _fp(alive, C.c_uint32), _fp(counts, C.c_uint32))
+    if rc:
+        raise MemoryError("oracle chem_grid")
+    return counts, pos, alive

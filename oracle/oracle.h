@@ -113,6 +113,12 @@ double orc_expected_dsb_local(const orc_dna *d, const float *lambda, const uint8
 double orc_dose_sum_ev(const uint32_t *dose, uint64_t n);
 void orc_dose_projection(const uint32_t *dose, uint32_t vc, int axis, float *proj);
 
+/* grid-hash chemistry backend (src/shaders/chemistry.wgsl, schedule.ts:38-46) on
+ * the first n rad_buf entries: final pos (n x 4: x, y, z, kind) and alive,
+ * counts[checkpoint][OH, eaq, H alive, H2O2 made, H2 made] at t = 0 and the
+ * 7 checkpoints */
+int orc_chem_grid(const float *rad, uint32_t n, uint64_t seed, float *pos, uint32_t *alive, uint32_t counts[8][5]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -24,3 +24,17 @@ def test_run_validation_sweep(tmp_path):
     assert back["tenKeV"]["primaryEnergyEv"] == 10000 and len(back["rows"]) == 8
     assert doc["tenKeV"]["chemistry1Us"]["G_OH"] > 0
     assert any("Validation run complete" in m for m in logs)
+
+
+@pytest.mark.gpu
+def test_run_validation_grid_backend_scores_indirect_ssb():
+    """With the 'gpu' backend the radical positions reach scoreIndirectSSB
+    (app.ts:178-180), unlike the IRT worker, whose SSB_ind stays 0."""
+    from wgdna import app
+    rows = app.run_validation(np=64, energies=[10000], chemBackend="gpu")
+    r = rows[0]
+    cr = r["result"]["chem_result"]
+    assert cr["timeline"][0]["label"] == "t=0" and len(cr["timeline"]) == 8
+    assert cr["chem_pos_final"].size == 4 * cr["chem_n"]
+    assert r["damage"] is not None and r["damage"]["ssb_ind"] >= 0
+    assert cr["timeline"][-1]["G_OH"] < cr["timeline"][0]["G_OH"]

@@ -8,6 +8,7 @@
 
 #include "common.cuh"
 
+#include "chemgrid.cuh"
 #include "dose.cuh"
 #include "irt.cuh"
 #include "scoring.cuh"
@@ -67,6 +68,14 @@ struct wgdna_ctx {
     uint8_t* d_hits_in = nullptr;
     double* d_dres = nullptr;
     bool have_lambda = false;
+    // grid-hash chemistry
+    float4 *d_cg_pos = nullptr, *d_cg_rad = nullptr;
+    uint32_t *d_cg_alive = nullptr, *d_cg_prod = nullptr, *d_cg_counts = nullptr;
+    int *d_cg_head = nullptr, *d_cg_next = nullptr;
+    wg::CgStep* d_cg_step = nullptr;
+    size_t cg_cap = 0, cg_rad_cap = 0;
+    cudaGraphExec_t cg_graph = nullptr;
+    wg::CgGraphKey cg_key{};
     unsigned long long last_rad_n = 0;
     // DNA target + scoring
     wgdna_dna_info dna{};
@@ -221,7 +230,9 @@ extern "C" void wgdna_destroy(wgdna_ctx* c) {
                     c->sc.info, c->sc.last_brk, c->sc.cnt0, c->sc.cnt1, c->sc.cs_in, c->sc.base, c->sc.u64,
                     c->sc.fib, c->d_px, c->d_py, c->d_pz, c->d_tb, c->d_sp, c->d_alive8, c->d_lst, c->d_lpos, c->d_evt, c->d_evab,
                     c->d_hov_t, c->d_hov_ab, c->d_track, c->d_toff, c->d_irt_cnt, c->d_pf, c->d_rec, c->d_tdel, c->d_curves, c->d_acc_tl, c->d_acc, c->d_maxpid,
-                    c->d_dose_in, c->d_lambda, c->d_hits_in, c->d_dres};
+                    c->d_dose_in, c->d_lambda, c->d_hits_in, c->d_dres, c->d_cg_pos, c->d_cg_rad, c->d_cg_alive,
+                    c->d_cg_prod, c->d_cg_counts, c->d_cg_head, c->d_cg_next, c->d_cg_step};
+    if (c->cg_graph) cudaGraphExecDestroy(c->cg_graph);
     for (void* p : ptrs) if (p) cudaFree(p);
     for (auto& ev : c->ev) if (ev) cudaEventDestroy(ev);
     if (c->own) cudaStreamDestroy(c->own);
@@ -883,5 +894,57 @@ extern "C" int wgdna_expected_dsb_local(wgdna_ctx* c, const float* lambda, const
     WG_CUDA_OK(launch_expected_dsb(dose_dna(c), c->d_lambda, dh, c->d_dres, c->stream));
     WG_CUDA_OK(cudaMemcpyAsync(dsb_expected, c->d_dres, 8, cudaMemcpyDeviceToHost, c->stream));
     WG_CUDA_OK(cudaStreamSynchronize(c->stream));
+    return WGDNA_OK;
+}
+
+// ------------------------------------------------------------------ grid-hash chemistry
+extern "C" int wgdna_chem_grid(wgdna_ctx* c, const float* rad, uint64_t rad_n, uint32_t n_therm, double E_eV,
+                               uint64_t seed, wgdna_chem_grid_result* out, float* pos, uint32_t* alive, uint64_t cap) {
+    if (!c || !out) { wg_set_error("wgdna_chem_grid: NULL argument"); return WGDNA_ERR_ARG; }
+    WG_CUDA_OK(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    const float4* src;
+    uint64_t n_all;
+    if (rad) {
+        n_all = rad_n;
+        if (rad_n > c->cg_rad_cap) { TRY(dalloc(&c->d_cg_rad, rad_n)); c->cg_rad_cap = rad_n; }
+        WG_CUDA_OK(cudaMemcpyAsync(c->d_cg_rad, rad, rad_n * 16, cudaMemcpyHostToDevice, s));
+        src = c->d_cg_rad;
+    } else {
+        if (!c->have_transport) { wg_set_error("wgdna_chem_grid: no rad_buf (pass one or run wgdna_transport)"); return WGDNA_ERR_STATE; }
+        n_all = c->last_rad_n;
+        src = c->d_rad;
+    }
+    const uint32_t n = (uint32_t)(n_all < wg::CG_CHEM_N ? n_all : wg::CG_CHEM_N);   // CHEM_N cap (schedule.ts:57)
+    memset(out, 0, sizeof *out);
+    if (n == 0) return WGDNA_OK;
+    if (n > c->cg_cap) {
+        TRY(dalloc(&c->d_cg_pos, n)); TRY(dalloc(&c->d_cg_alive, n)); TRY(dalloc(&c->d_cg_next, n));
+        c->cg_cap = n;
+    }
+    if (!c->d_cg_head) {
+        TRY(dalloc(&c->d_cg_head, wg::CG_HASH_SIZE)); TRY(dalloc(&c->d_cg_prod, 2));
+        TRY(dalloc(&c->d_cg_counts, 40)); TRY(dalloc(&c->d_cg_step, 1));
+    }
+    wg::CgArgs a{src, n, (uint32_t)seed, (uint32_t)(seed >> 32), c->d_cg_pos, c->d_cg_alive, c->d_cg_head,
+                 c->d_cg_next, c->d_cg_prod, c->d_cg_counts, c->d_cg_step};
+    WG_CUDA_OK(cudaEventRecord(c->ev[4], s));
+    WG_CUDA_OK(wg::cg_run(a, s, &c->cg_graph, &c->cg_key));
+    WG_CUDA_OK(cudaEventRecord(c->ev[5], s));
+    uint32_t counts[40];
+    WG_CUDA_OK(cudaMemcpyAsync(counts, c->d_cg_counts, sizeof counts, cudaMemcpyDeviceToHost, s));
+    if (pos && cap >= n) WG_CUDA_OK(cudaMemcpyAsync(pos, c->d_cg_pos, (size_t)n * 16, cudaMemcpyDeviceToHost, s));
+    if (alive && cap >= n) WG_CUDA_OK(cudaMemcpyAsync(alive, c->d_cg_alive, (size_t)n * 4, cudaMemcpyDeviceToHost, s));
+    WG_CUDA_OK(cudaStreamSynchronize(s));
+    cudaEventElapsedTime(&out->ms, c->ev[4], c->ev[5]);
+    out->chem_n = n;
+    // G per 100 eV of the deposited energy carried by the chem_n radicals (schedule.ts:218-227)
+    out->deposited_eV = (double)n_therm * E_eV * ((double)n / (double)n_all);
+    const double per100 = out->deposited_eV / 100;
+    for (int k = 0; k < 8; ++k)
+        for (int q = 0; q < 5; ++q) {
+            out->counts[k][q] = counts[5 * k + q];
+            out->G[k][q] = per100 > 0 ? counts[5 * k + q] / per100 : 0;
+        }
     return WGDNA_OK;
 }

@@ -25,7 +25,7 @@ EXPORTS = ["wgdna_default_cfg", "wgdna_create", "wgdna_destroy", "wgdna_last_err
            "wgdna_track_descriptors", "wgdna_surrogate_init", "wgdna_surrogate_params", "wgdna_surrogate_norm",
            "wgdna_surrogate_load", "wgdna_surrogate_train", "wgdna_surrogate_grad", "wgdna_surrogate_predict",
            "wgdna_surrogate_chemistry", "wgdna_dose_sum", "wgdna_dose_projection", "wgdna_score_voxel_ssb",
-           "wgdna_expected_dsb_local"]
+           "wgdna_expected_dsb_local", "wgdna_chem_grid"]
 SG_IN, SG_OUT, SG_NPARAM = 64, 80, 51664
 
 
@@ -64,6 +64,11 @@ class IrtResult(C.Structure):
                 ("chem_n", C.c_uint64), ("ms", C.c_float),
                 ("ms_load", C.c_float), ("ms_pairing", C.c_float), ("ms_events", C.c_float),
                 ("device_error", C.c_uint32)]
+
+
+class ChemGridResult(C.Structure):
+    _fields_ = [("counts", (C.c_uint32 * 5) * 8), ("G", (C.c_double * 5) * 8), ("chem_n", C.c_uint64),
+                ("deposited_eV", C.c_double), ("ms", C.c_float)]
 
 
 class DnaInfo(C.Structure):
@@ -132,6 +137,8 @@ def lib():
         "wgdna_dose_projection": (C.c_int, [vp, vp, C.c_int, vp]),
         "wgdna_score_voxel_ssb": (C.c_int, [vp, vp, C.c_double, vp, P(C.c_double)]),
         "wgdna_expected_dsb_local": (C.c_int, [vp, vp, vp, P(C.c_double)]),
+        "wgdna_chem_grid": (C.c_int, [vp, vp, C.c_uint64, C.c_uint32, C.c_double, C.c_uint64, P(ChemGridResult),
+                                      vp, vp, C.c_uint64]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -66,10 +66,11 @@ def run_validation(np=4096, boxNm=15000.0, ceEV=7.4, log=_nolog, chemBackend=DEF
     """runValidation (app.ts:91-161): the ESTAR sweep, chemistry + damage at 10 keV.
 
     Returns one row per energy (the reference paints them into a table).
-    chemBackend 'worker' runs the CUDA IRT; 'none' skips chemistry; 'gpu' (the
-    reference's grid-hash backend) is not part of this path and raises."""
-    if chemBackend not in ("worker", "none"):
-        raise ValueError(f"chemBackend {chemBackend!r}: only 'worker' (IRT) and 'none' are built")
+    chemBackend 'worker' runs the CUDA IRT; 'gpu' the grid-hash diffusion-reaction
+    backend (its radical positions feed the indirect SSB scoring); 'none'
+    skips chemistry (src/chemistry/backend.ts:16-18)."""
+    if chemBackend not in ("worker", "gpu", "none"):
+        raise ValueError(f"chemBackend {chemBackend!r}: expected 'worker', 'gpu' or 'none'")
     ctx = ensure_pipelines(np, log)
     log(f"Running {np} primaries at {len(ESTAR)} energies, box={boxNm}nm, cutoff={ceEV}eV", "data")
     dna = build_dna_target(DNA_LENGTH_NM, DNA_GRID_N, DNA_SPACING_NM)
@@ -78,6 +79,9 @@ def run_validation(np=4096, boxNm=15000.0, ceEV=7.4, log=_nolog, chemBackend=DEF
     rng = make_ssb_rng()
     if chemBackend == "none":
         chem = None
+    elif chemBackend == "gpu":
+        from .chemistry import run_chemistry_grid
+        chem = lambda rb, rn, nt, e: run_chemistry_grid(ctx, nt, e, rad_n=rn)    # device rad_buf
     elif device_chemistry:
         chem = "device"
     else:

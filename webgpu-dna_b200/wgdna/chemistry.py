@@ -1,6 +1,7 @@
 """Phase C: Karamitros 9-reaction IRT (src/chemistry/worker.ts:32-87 +
 public/irt-worker.js:370-699), run by the CUDA kernel through the C ABI."""
 import ctypes as C
+import time
 
 import numpy as np
 
@@ -46,6 +47,44 @@ def run_chemistry_device(ctx, n_therm, E_eV, log=None, seed=1):
     r = _lib.IrtResult()
     _lib.check("wgdna_irt", _lib.lib().wgdna_irt(ctx.h, int(n_therm), float(E_eV), int(seed), C.byref(r)))
     return _chem_result(r, r.chem_n, log)
+
+
+GRID_LABELS = ("t=0", "1 ps", "10 ps", "100 ps", "1 ns", "10 ns", "100 ns", "1 μs")
+GRID_T_NS = (0.0, 0.001, 0.01, 0.1, 1.0, 10.0, 100.0, 1000.0)
+
+
+def run_chemistry_grid(ctx, n_therm, E_eV, rad_buf=None, rad_n=None, seed=1, log=None):
+    """runChemistry of the 'gpu' backend (src/chemistry/schedule.ts:48-247): the
+    grid-hash diffusion-reaction schedule on the device rad_buf of the last
+    transport (or on a host rad_buf), with the final radical positions and
+    alive flags that scoreIndirectSSB consumes."""
+    L = _lib.lib()
+    r = _lib.ChemGridResult()
+    if rad_buf is not None:
+        rad = np.ascontiguousarray(np.asarray(rad_buf, dtype=np.float32).reshape(-1, 4)[: int(rad_n)])
+        n_all = rad.shape[0]
+        src = _lib.ptr(rad)
+    else:
+        rad, n_all, src = None, 0, None
+    cap = min(n_all if rad is not None else int(rad_n or 8_000_000), 8_000_000)
+    # sizes are known after the call; ask for positions with a buffer of the cap
+    k = C.c_uint64()
+    pos = np.zeros((cap, 4), np.float32) if cap else np.zeros((1, 4), np.float32)
+    alive = np.zeros(max(cap, 1), np.uint32)
+    t0 = time.perf_counter()
+    _lib.check("wgdna_chem_grid", L.wgdna_chem_grid(ctx.h, src, n_all, int(n_therm), float(E_eV), int(seed),
+                                                    C.byref(r), _lib.ptr(pos), _lib.ptr(alive), pos.shape[0]))
+    n = int(r.chem_n)
+    timeline = []
+    for kk in range(8):
+        c = r.counts[kk]
+        g = r.G[kk]
+        timeline.append({"label": GRID_LABELS[kk], "t_ns": GRID_T_NS[kk],
+                         "G_OH": g[0], "G_eaq": g[1], "G_H": g[2], "G_H2O2": g[3], "G_H2": g[4],
+                         "alive_OH": c[0], "alive_eaq": c[1], "alive_H": c[2], "prod_H2O2": c[3], "prod_H2": c[4]})
+    return {"chem_n": n, "t_wall": (time.perf_counter() - t0) * 1000.0, "timeline": timeline,
+            "chem_pos_final": pos[:n].reshape(-1), "chem_alive_final": alive[:n], "deposited_eV": r.deposited_eV,
+            "ms": r.ms}
 
 
 runChemistryWorker = run_chemistry_worker
