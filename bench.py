@@ -566,7 +566,7 @@ def run_surrogate(args):
 
 def run_sweep(args):
     """DNA-damage sweep: primaries at 1, 3 and 10 keV in batches of 4096
-    through transport, the surrogate chemistry (the IRT judging 1 % of the
+    through transport, the surrogate chemistry (the IRT checking 1 % of the
     batches) and direct SSB + DSB scoring (10 bp window) on the 21 x 21 fibre
     grid; yields per Gy and per primary."""
     import ctypes as C
@@ -590,7 +590,7 @@ def run_sweep(args):
             ir = _lib.IrtResult()
             dep = 0.0
             n_ssb = n_dsb = 0
-            judge = []
+            checks = []
             Gsum = np.zeros(80)
             ms_tr = ms_sg = ms_sc = 0.0
             t0 = time.perf_counter()
@@ -602,14 +602,14 @@ def run_sweep(args):
                 Gc = np.zeros(80)
                 ms = C.c_float()
                 _lib.check("chem", L.wgdna_surrogate_chemistry(ctx.h, _lib.ptr(Gc), C.byref(ms)))
-                if b % 100 == 50 or nb < 100 and b == nb // 2:                      # the IRT judges 1 %
+                if b % 100 == 50 or nb < 100 and b == nb // 2:                      # the IRT checks 1 %
                     L.wgdna_irt_record_curves(ctx.h, 1)
                     _lib.check("irt", L.wgdna_irt(ctx.h, st.n_therm, E, b + 1, C.byref(ir)))
                     L.wgdna_irt_record_curves(ctx.h, 0)
                     # 1 ps, 100 ps, 10 ns and 1 us are both IRT checkpoints and curve times
                     gi = np.array(ir.G)[[0, 2, 4, 6]]
                     gs = Gc.reshape(16, 5)[[0, 5, 10, 15]]
-                    judge.append(float((np.abs(gs - gi) / np.maximum(gi, 1e-12))[gi > 0.05].max()))
+                    checks.append(float((np.abs(gs - gi) / np.maximum(gi, 1e-12))[gi > 0.05].max()))
                 _lib.check("score", L.wgdna_score(ctx.h, 0x12345678, C.byref(ssb), C.byref(dsb)))
                 dep += st.dep_eV_f64
                 n_ssb += ssb.ssb
@@ -624,7 +624,7 @@ def run_sweep(args):
                             "DSB_per_Gy_Gbp": n_dsb / (dose * gbp) if dose > 0 else 0.0,
                             "SSB_per_Gy_Gbp": n_ssb / (dose * gbp) if dose > 0 else 0.0,
                             "G_1us": list(np.round((Gsum / (n_per * E)).reshape(16, 5)[15], 4)),
-                            "irt_judge_max_rel_err": max(judge) if judge else None, "irt_judged_batches": len(judge),
+                            "irt_check_max_rel_err": max(checks) if checks else None, "irt_checked_batches": len(checks),
                             "device_ms": {"transport": ms_tr, "surrogate": ms_sg, "scoring": ms_sc},
                             "primaries_per_s_device": n_per / ((ms_tr + ms_sg + ms_sc) / 1000.0),
                             "primaries_per_s_wall": n_per / wall}

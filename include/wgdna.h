@@ -209,7 +209,7 @@ int wgdna_expected_dsb_local(wgdna_ctx *ctx, const float *lambda, const uint8_t 
  * mapping a track descriptor to the track's G(t) (per 100 eV of the track's
  * energy) at the 16 curve times of wgdna_irt_curves, species-major within a
  * time: out[5 k + s], s = OH, eaq, H, H2O2, H2.  The IRT stays the reference
- * and the judge: the model is trained on the IRT's own curves.
+ * and the check: the model is trained on the IRT's own curves.
  *
  * Parameters (WGDNA_SG_NPARAM floats): W1 [128][64], b1 [128], W2 [128][128],
  * b2, W3 [128][128], b3, W4 [80][128], b4 [80].  Standardisation

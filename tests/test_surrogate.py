@@ -105,7 +105,7 @@ def test_irt_curves_bit_exact(ctx):
 
 @pytest.mark.gpu
 def test_trained_surrogate_against_irt(ctx):
-    """Train on the IRT's own curves at 3 and 10 keV, then judge a held-out
+    """Train on the IRT's own curves at 3 and 10 keV, then check a held-out
     batch: the surrogate's G(1 us) against the IRT's, and its time against the
     IRT's on the same tracks (what the network gains over the method alone)."""
     from wgdna import surrogate as S

@@ -10,7 +10,7 @@ import sys
 import numpy as np
 import pytest
 
-from conftest import PKG, REFERENCE
+from conftest import PKG
 
 DATA = os.path.join(PKG, "data")
 
@@ -52,13 +52,17 @@ def test_table_inventory():
     assert int(T["N_AE"][0]) == 25 and int(T["N_AC"][0]) == 25 and int(T["N_VIB"][0]) == 38
 
 
-@pytest.mark.skipif(not os.path.exists(os.path.join(REFERENCE, "public", "cross_sections.wgsl")),
-                    reason="reference checkout not mounted")
-def test_blob_regenerates_bit_identical(tmp_path):
-    """Re-parse the reference's WGSL and compare every array bit for bit."""
+def _wgsl_source():
     sys.path.insert(0, DATA)
     import gen_tables
-    text = open(os.path.join(REFERENCE, "public", "cross_sections.wgsl")).read()
+    return gen_tables.DEFAULT_SRC
+
+
+@pytest.mark.skipif(not os.path.exists(_wgsl_source()), reason="reference checkout not mounted")
+def test_blob_regenerates_bit_identical(tmp_path):
+    """Re-parse the reference's WGSL and compare every array bit for bit."""
+    import gen_tables
+    text = open(_wgsl_source()).read()
     arrays = gen_tables.parse_wgsl(text)
     assert gen_tables.build_blob(arrays) == BLOB
     for name, a in arrays:

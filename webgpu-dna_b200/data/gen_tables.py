@@ -38,7 +38,7 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_SRC = "/root/reference/public/cross_sections.wgsl"
+DEFAULT_SRC = os.environ.get("WGDNA_REFERENCE_WGSL", "/root/reference/public/cross_sections.wgsl")
 MAGIC = b"WGDNAXS1"
 ENTRY_FMT = "<24sIIII"
 

@@ -5,7 +5,7 @@ The model (csrc/surrogate.cu) maps a track descriptor (64 floats, computed on
 the device from the track's rad_buf entries) to the track's G(t) at the 16
 curve times t_k = 10^(-3 + 0.4 k) ns for OH, e-aq, H, H2O2 and H2.  Training
 targets are the IRT's own per-track curves (wgdna_irt_curves) divided by the
-track's energy / 100 eV.  The IRT stays the judge: ``chemistry`` falls back
+track's energy / 100 eV.  The IRT stays the reference: ``chemistry`` falls back
 to it when a batch's descriptors leave the training range.
 """
 import ctypes as C
