@@ -102,7 +102,7 @@ struct wgdna_ctx {
     uint32_t* d_evab = nullptr;
     double* d_hov_t = nullptr;
     uint32_t* d_hov_ab = nullptr;
-    uint32_t* d_track = nullptr;          // 10 per track: tn, th2, ttiles, tev, tlc[6]
+    uint32_t* d_track = nullptr;          // 11 per track: tn, th2, ttiles, tev, tlc[6], order
     unsigned long long* d_toff = nullptr;
     uint32_t* d_irt_cnt = nullptr;
     double* d_acc_tl = nullptr;
@@ -266,6 +266,7 @@ static IArgs make_iargs(wgdna_ctx* c, uint32_t nseg, uint64_t seed) {
     const size_t T = c->irt_tracks;
     a.tn = c->d_track; a.th2 = c->d_track + T; a.ttiles = c->d_track + 2 * T; a.tev = c->d_track + 3 * T;
     a.tlc = c->d_track + 4 * T;
+    a.order = c->d_track + 10 * T;
     a.toff = c->d_toff;
     a.pf = c->d_pf; a.rec = c->d_rec; a.tdel = c->d_tdel;
     a.hov_t = c->d_hov_t; a.hov_ab = c->d_hov_ab; a.hcap = c->irt_hcap;
@@ -414,7 +415,7 @@ static int irt_ensure(wgdna_ctx* c, uint32_t nseg, uint64_t rad_n, uint32_t cap)
         c->irt_pf_slots = slots;
     }
     if (nseg > c->irt_tracks) {
-        TRY(dalloc(&c->d_track, 10 * (size_t)nseg)); TRY(dalloc(&c->d_toff, (size_t)nseg + 1));
+        TRY(dalloc(&c->d_track, 11 * (size_t)nseg)); TRY(dalloc(&c->d_toff, (size_t)nseg + 1));
         TRY(dalloc(&c->d_tdel, (size_t)nseg));
         c->irt_tracks = nseg;
     }

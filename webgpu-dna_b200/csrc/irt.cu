@@ -753,10 +753,11 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
     unsigned long long n_pairs = 0;
     __syncwarp();
     for (;;) {
-        uint32_t p = 0;
-        if (lane == 0) p = atomicAdd(&A.counters[2], 1u);
-        p = __shfl_sync(FULL, p, 0);
-        if (p >= A.nseg) break;
+        uint32_t k = 0;
+        if (lane == 0) k = atomicAdd(&A.counters[2], 1u);
+        k = __shfl_sync(FULL, k, 0);
+        if (k >= A.nseg) break;
+        const uint32_t p = A.order[k];                 // largest tracks first
         const uint32_t n = A.tn[p];
         if (n == 0) continue;
         const uint32_t pid = A.pid_base + p;
@@ -1041,6 +1042,35 @@ static int blocks_for(const void* k, int device) {
     return sms * per;
 }
 
+// Order of the event kernel's tracks: by species count, largest first (a
+// bucket sort in one block), so the longest event chains start early and the
+// last wave holds the short ones.
+__global__ void __launch_bounds__(1024) k_track_order(const uint32_t* tn, uint32_t nseg, uint32_t* order) {
+    constexpr int NB = 512;
+    __shared__ uint32_t cnt[NB], off[NB];
+    __shared__ uint32_t smax;
+    if (threadIdx.x == 0) smax = 0;
+    for (int b = threadIdx.x; b < NB; b += blockDim.x) cnt[b] = 0;
+    __syncthreads();
+    uint32_t m = 0;
+    for (uint32_t p = threadIdx.x; p < nseg; p += blockDim.x) m = max(m, tn[p]);
+    atomicMax(&smax, m);
+    __syncthreads();
+    const uint32_t mx = smax > 0 ? smax : 1;
+    for (uint32_t p = threadIdx.x; p < nseg; p += blockDim.x)
+        atomicAdd(&cnt[(uint32_t)(((unsigned long long)(mx - min(tn[p], mx)) * (NB - 1)) / mx)], 1u);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t a = 0;
+        for (int b = 0; b < NB; ++b) { off[b] = a; a += cnt[b]; }
+    }
+    __syncthreads();
+    for (uint32_t p = threadIdx.x; p < nseg; p += blockDim.x) {
+        const uint32_t b = (uint32_t)(((unsigned long long)(mx - min(tn[p], mx)) * (NB - 1)) / mx);
+        order[atomicAdd(&off[b], 1u)] = p;
+    }
+}
+
 int irt_warps(int device) { return blocks_for((const void*)k_irt_loop, device) * (IB / 32); }
 
 // tile prefix: the scan of transport.cu
@@ -1054,6 +1084,7 @@ cudaError_t launch_irt(const IArgs& a, int device, cudaStream_t s, cudaEvent_t* 
     if (ev) cudaEventRecord(ev[0], s);
     k_irt_init<<<blocks_for((const void*)k_irt_init, device), IB, 0, s>>>(a);
     if (ev) cudaEventRecord(ev[1], s);
+    k_track_order<<<1, 1024, 0, s>>>(a.tn, a.nseg, a.order);
     k_irt_loop<<<blocks_for((const void*)k_irt_loop, device), IB, 0, s>>>(a);
     return cudaGetLastError();
 }

@@ -36,6 +36,7 @@ struct IArgs {
     uint32_t* ev_ab;                     // packed (a << 16) | b
     uint32_t *tn, *th2, *ttiles, *tev, *tlc;   // per track: particles, H2 markers, tiles, events, 6 list lengths
     unsigned long long* toff;            // nseg + 1: prefix of ttiles
+    uint32_t* order;                     // nseg: tracks in the order the event kernel takes them
     // per-warp heap overflow of the event kernel
     double* hov_t;
     uint32_t* hov_ab;
