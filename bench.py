@@ -44,7 +44,7 @@ WORKLOAD = ("4096 x 10 keV e- in liquid water, box +-15 um, cutoff 7.5 eV, Philo
 CPU_SAMPLE_PRIMARIES = 512
 # library kernels per step: transport 1, rad_buf canonical order 5 (histogram,
 # scan, scatter, segment sort, reduce), IRT 6 (segment max, load, scan,
-# pairing, events), scoring 5 (prep, tiles, tile scan, apply, cluster)
+# pairing, order, events), scoring 5 (prep, tiles, tile scan, apply, cluster)
 LAUNCHES_PER_STEP = 17
 
 
