@@ -166,7 +166,7 @@ def run_native(args, ws, rank, local):
     import numpy as np
     import torch
     import wgdna
-    from wgdna import _lib
+    from wgdna import _lib, sharded
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
@@ -185,18 +185,21 @@ def run_native(args, ws, rank, local):
     ir = _lib.IrtResult()
     ssb = _lib.SsbResult()
     dsb = _lib.DsbResult()
-    summary = torch.zeros(64, dtype=torch.float64, device=dev)
+
+    job = {}
 
     def step_device():
         _lib.check("wgdna_transport", L.wgdna_transport(ctx.h, C.byref(p), C.byref(st)))
         _lib.check("wgdna_irt", L.wgdna_irt(ctx.h, st.n_therm, E_EV, args.seed + 1, C.byref(ir)))
-        _lib.check("wgdna_score", L.wgdna_score(ctx.h, 0x12345678, C.byref(ssb), C.byref(dsb)))
-        if ws > 1:
-            vals = [float(st.n_therm), float(st.dep_units), float(dsb.dsb), float(ssb.ssb)] + \
-                   [float(x) for x in np.array(ir.counts).reshape(-1)]
-            with torch.cuda.stream(stream):
-                summary[:len(vals)].copy_(torch.tensor(vals, dtype=torch.float64), non_blocking=True)
-                torch.distributed.all_reduce(summary)
+        if ws == 1:
+            _lib.check("wgdna_score", L.wgdna_score(ctx.h, 0x12345678, C.byref(ssb), C.byref(dsb)))
+            return
+        # exchange steps of the sharded job: dose grid and IRT counts summed, direct
+        # SSB scored exactly as on one device (draw counts all-gathered, hits MAX-reduced)
+        with torch.cuda.stream(stream):
+            job["ssb"], job["dsb"], job["reach"], job["counts"] = sharded.device_step_exchange(
+                ctx, torch.distributed, 0x12345678, dev,
+                irt_counts=np.concatenate([np.array(ir.counts).reshape(-1), [float(st.n_therm)]]))
 
     # pinned host buffers for the end-to-end path
     E_host = torch.full((NPr,), E_EV, dtype=torch.float32, pin_memory=True)
@@ -321,6 +324,7 @@ def run_native(args, ws, rank, local):
                          "alg_bytes": int(alg),
                          "peak_source": "fallback" if pk.get("fallback") else "measured"},
             "clocks": clocks,
+            "job": {"ssb": job.get("ssb"), "dsb": job.get("dsb"), "in_reach": job.get("reach")} if ws > 1 else None,
             "work": {"rad_n": int(R), "sec_n": int(S), "steps": int(st.steps), "irt_pairs": int(ir.n_pairs),
                      "irt_events": int(ir.n_events), "irt_init_events": int(Ei), "irt_species": int(Np),
                      "dose_atomics": int(D), "ssb": int(ssb.ssb), "dsb": int(dsb.dsb)},

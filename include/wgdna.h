@@ -241,6 +241,31 @@ int wgdna_surrogate_predict(wgdna_ctx *ctx, const float *X, uint64_t n, float *G
  * surrogate's G(t) of the whole batch, G[16][5]; ms = device time. */
 int wgdna_surrogate_chemistry(wgdna_ctx *ctx, double *G, float *ms);
 
+/* ---------------------------------------------------------------- sharded runs */
+/* One process per GPU, each with its block of primary ids (pid_base).  The
+ * exchange steps need the context's device buffers: the dose grid (summed
+ * over ranks), the hit bytes (OR-ed: MAX over ranks) and, for the exact
+ * sharded direct-SSB scoring, a scoring pass that only reports its LCG draws
+ * and leaves the hit bytes on the device, then clustering of the reduced
+ * hits.  No reference counterpart: the reference runs on one device. */
+typedef struct {
+    uint32_t *dose;             /* vc^3 words */
+    uint64_t dose_words;
+    uint8_t *hits;              /* 2 * n_bp bytes (allocation rounded up to 4) */
+    uint64_t hits_bytes;
+    float *rad;                 /* canonical rad_buf of the last transport: rad_n x 4 */
+    uint64_t rad_n;
+    float *results;             /* n_primaries x 8 */
+    uint32_t n_primaries;
+    void *stream;               /* the context's cudaStream_t */
+} wgdna_device_view;
+int wgdna_device_views(wgdna_ctx *ctx, wgdna_device_view *v);
+/* scoreDirectSSB_events of the last transport's rad_buf into zeroed device
+ * hits: SSB counts, in_reach (= LCG draws) and the LCG state after them. */
+int wgdna_score_draws(wgdna_ctx *ctx, uint32_t lcg_state, wgdna_ssb_result *ssb);
+/* clusterDSB of the device hit bytes (after the caller's reduction). */
+int wgdna_cluster_device(wgdna_ctx *ctx, wgdna_dsb_result *dsb);
+
 /* Direct SSB scoring that allocates nothing.  No counterpart in the reference:
  * it serves callers that cannot call cudaMalloc (a host running under another
  * framework's memory pool or a fixed device-memory budget, or code that must

@@ -949,3 +949,33 @@ extern "C" int wgdna_chem_grid(wgdna_ctx* c, const float* rad, uint64_t rad_n, u
         }
     return WGDNA_OK;
 }
+
+// ------------------------------------------------------------------ sharded runs
+extern "C" int wgdna_device_views(wgdna_ctx* c, wgdna_device_view* v) {
+    if (!c || !v) { wg_set_error("wgdna_device_views: NULL argument"); return WGDNA_ERR_ARG; }
+    memset(v, 0, sizeof *v);
+    v->dose = c->d_dose;
+    v->dose_words = (uint64_t)c->cfg.vc * c->cfg.vc * c->cfg.vc;
+    v->hits = c->d_hits;
+    v->hits_bytes = (uint64_t)c->dna.n_bp * 2;
+    v->rad = reinterpret_cast<float*>(c->d_rad);
+    v->rad_n = c->have_transport ? c->last_rad_n : 0;
+    v->results = c->d_results;
+    v->n_primaries = c->last_np;
+    v->stream = c->stream;
+    return WGDNA_OK;
+}
+
+extern "C" int wgdna_score_draws(wgdna_ctx* c, uint32_t lcg_state, wgdna_ssb_result* ssb) {
+    if (!c) { wg_set_error("wgdna_score_draws: NULL context"); return WGDNA_ERR_ARG; }
+    if (!c->have_transport) { wg_set_error("wgdna_score_draws: no transport result in the context"); return WGDNA_ERR_STATE; }
+    WG_CUDA_OK(cudaSetDevice(c->device));
+    TRY(hits_in(c, nullptr));
+    return score_dev(c, c->d_rad, nullptr, c->last_rad_n, 0.15, 1, lcg_state, ssb);
+}
+
+extern "C" int wgdna_cluster_device(wgdna_ctx* c, wgdna_dsb_result* dsb) {
+    if (!c) { wg_set_error("wgdna_cluster_device: NULL context"); return WGDNA_ERR_ARG; }
+    WG_CUDA_OK(cudaSetDevice(c->device));
+    return cluster_dev(c, dsb);
+}

@@ -25,7 +25,8 @@ EXPORTS = ["wgdna_default_cfg", "wgdna_create", "wgdna_destroy", "wgdna_last_err
            "wgdna_track_descriptors", "wgdna_surrogate_init", "wgdna_surrogate_params", "wgdna_surrogate_norm",
            "wgdna_surrogate_load", "wgdna_surrogate_train", "wgdna_surrogate_grad", "wgdna_surrogate_predict",
            "wgdna_surrogate_chemistry", "wgdna_dose_sum", "wgdna_dose_projection", "wgdna_score_voxel_ssb",
-           "wgdna_expected_dsb_local", "wgdna_chem_grid"]
+           "wgdna_expected_dsb_local", "wgdna_chem_grid", "wgdna_device_views", "wgdna_score_draws",
+           "wgdna_cluster_device"]
 SG_IN, SG_OUT, SG_NPARAM = 64, 80, 51664
 
 
@@ -69,6 +70,12 @@ class IrtResult(C.Structure):
 class ChemGridResult(C.Structure):
     _fields_ = [("counts", (C.c_uint32 * 5) * 8), ("G", (C.c_double * 5) * 8), ("chem_n", C.c_uint64),
                 ("deposited_eV", C.c_double), ("ms", C.c_float)]
+
+
+class DeviceView(C.Structure):
+    _fields_ = [("dose", C.c_void_p), ("dose_words", C.c_uint64), ("hits", C.c_void_p), ("hits_bytes", C.c_uint64),
+                ("rad", C.c_void_p), ("rad_n", C.c_uint64), ("results", C.c_void_p), ("n_primaries", C.c_uint32),
+                ("stream", C.c_void_p)]
 
 
 class DnaInfo(C.Structure):
@@ -139,6 +146,9 @@ def lib():
         "wgdna_expected_dsb_local": (C.c_int, [vp, vp, vp, P(C.c_double)]),
         "wgdna_chem_grid": (C.c_int, [vp, vp, C.c_uint64, C.c_uint32, C.c_double, C.c_uint64, P(ChemGridResult),
                                       vp, vp, C.c_uint64]),
+        "wgdna_device_views": (C.c_int, [vp, P(DeviceView)]),
+        "wgdna_score_draws": (C.c_int, [vp, C.c_uint32, P(SsbResult)]),
+        "wgdna_cluster_device": (C.c_int, [vp, P(DsbResult)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -86,3 +86,61 @@ def sharded_score(dist, score_fn, rad_local, lcg_state, n_bp, group=None):
     total = sum(counts)
     return {"hits": hits_all, "ssb_count": ssb0 + ssb1, "ssb0": ssb0, "ssb1": ssb1, "in_reach": total,
             "candidates": sum(cands), "lcg_state": lcg_jump(lcg_state, total), "offset": offset}
+
+
+# ---------------------------------------------------------------- device path
+class _CudaArray:
+    """A device buffer of the library seen by torch (zero copy)."""
+
+    def __init__(self, ptr, n, typestr):
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 3}
+
+
+def device_tensor(ptr, n, typestr, device):
+    import torch
+    return torch.as_tensor(_CudaArray(ptr, n, typestr), device=device)
+
+
+def device_step_exchange(ctx, dist, lcg_state, device, irt_counts=None, group=None):
+    """The exchange steps of a sharded pipeline step on the device, after every
+    rank ran wgdna_transport (and wgdna_irt) on its block of primaries:
+
+      * dose grid: NCCL sum (the u32 grid summed as int32 wraps the same way);
+      * IRT checkpoint counts: sum;
+      * direct SSB scoring, exactly as on one device: each rank scores its
+        rad_buf once to learn its LCG draws, the draws are all-gathered,
+        each rank scores again from the LCG state advanced past the lower ranks'
+        draws, the hit bytes are MAX-reduced and every rank clusters DSBs on
+        the combined hits.
+
+    Returns (ssb, dsb, in_reach, counts) of the whole job."""
+    import ctypes as C
+    import numpy as np
+    import torch
+    from . import _lib
+    L = _lib.lib()
+    v = _lib.DeviceView()
+    _lib.check("wgdna_device_views", L.wgdna_device_views(ctx.h, C.byref(v)))
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    dose = device_tensor(v.dose, v.dose_words, "<i4", device)
+    dist.all_reduce(dose, group=group)
+    counts = None
+    if irt_counts is not None:
+        t = torch.tensor(np.asarray(irt_counts, np.float64).reshape(-1), device=device)
+        dist.all_reduce(t, group=group)
+        counts = t.cpu().numpy()
+    s1 = _lib.SsbResult()
+    _lib.check("wgdna_score_draws", L.wgdna_score_draws(ctx.h, lcg_state, C.byref(s1)))
+    n = torch.tensor([int(s1.in_reach)], dtype=torch.int64, device=device)
+    alln = [torch.zeros_like(n) for _ in range(world)]
+    dist.all_gather(alln, n, group=group)
+    draws = [int(x.item()) for x in alln]
+    s2 = _lib.SsbResult()
+    _lib.check("wgdna_score_draws", L.wgdna_score_draws(ctx.h, lcg_jump(lcg_state, sum(draws[:rank])), C.byref(s2)))
+    hits = device_tensor(v.hits, v.hits_bytes, "|u1", device)
+    dist.all_reduce(hits, op=dist.ReduceOp.MAX, group=group)
+    d = _lib.DsbResult()
+    _lib.check("wgdna_cluster_device", L.wgdna_cluster_device(ctx.h, C.byref(d)))
+    return int(d.ssb0 + d.ssb1), int(d.dsb), sum(draws), counts
