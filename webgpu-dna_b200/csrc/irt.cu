@@ -109,6 +109,14 @@ __device__ __forceinline__ float erfcx_f(float z) {
 //   <= 1.13 and <= 1/z); with the 3.3e-7 of erfcx_f (8e-7 with the fast
 //   exp) the prefactor Q is known to 4e-6, taken as 2e-5, 1 - Q to that
 //   plus 1e-6;
+//   for z >= 6 and b >= 0, where 1 - Q cancels, 1 - Q itself: with
+//   beta = (b/sqrt(X))/z, Q = (1 - beta) S and erfcx(z) = S/(z sqrt(pi)),
+//   S = 1 - h s (h = 1/(2z^2), s the asymptotic series of erfcx_f), so
+//   1 - Q = beta + (1 - beta) h s, a sum of two non-negative terms known to
+//   1.7e-6 and 4.2e-6 relative (1/z correctly rounded; the f32 series
+//   within 2.2e-7 of h s); taken as 2e-5.  The f64 1 - Q it must bound
+//   carries the rounding of Q near 1 (about 7 ulp, the continued fraction
+//   of erfcx_pos within 2.2e-16), so 1e-14 is added on both sides;
 // and decides when U2 (or U2 M against lambdax X) lies outside the bracket
 // with a further 1e-6 (3e-6) margin.  Trials inside the bracket, near
 // X = 2b/a, with e below exp(-80) in case B, z < 0, or a zero draw are
@@ -145,8 +153,18 @@ __device__ __noinline__ double pdc_warp(uint32_t i, uint32_t j, uint32_t pid, ui
                 const float sx = xf * rs;
                 const float zf = bf * rs + af * sx;
                 if (zf >= 0.0f) {
-                    const float Q = af * 1.7724539f * sx * erfcx_f(zf);
-                    const float flo = 1.0f - Q * 1.00002f - 1e-6f, fhi = 1.0f - Q * 0.99998f + 1e-6f;
+                    float flo, fhi;
+                    if (zf >= 6.0f && bf >= 0.0f) {
+                        const float iz = __frcp_rn(zf), h = 0.5f * iz * iz;
+                        float s = 1.0f - 13.0f * h;
+                        s = 1.0f - 11.0f * h * s; s = 1.0f - 9.0f * h * s; s = 1.0f - 7.0f * h * s;
+                        s = 1.0f - 5.0f * h * s; s = 1.0f - 3.0f * h * s;
+                        const float omq = fmaf(af * sx * iz, h * s, bf * rs * iz);
+                        flo = omq * 0.99998f - 1e-14f; fhi = omq * 1.00002f + 1e-14f;
+                    } else {
+                        const float Q = af * 1.7724539f * sx * erfcx_f(zf);
+                        flo = 1.0f - Q * 1.00002f - 1e-6f; fhi = 1.0f - Q * 0.99998f + 1e-6f;
+                    }
                     const double Llo = (double)(elo * fmaxf(flo, 0.0f)) * (1.0 - 1e-6);
                     const double Lhi = (double)(ehi * fmaxf(fhi, 0.0f)) * (1.0 + 1e-6) + 1e-37;
                     if (ca) st = U2 <= Llo ? 1 : (U2 > Lhi ? 0 : 2);
