@@ -471,7 +471,7 @@ __device__ __forceinline__ bool pair_maybe(const IrtConst& C, int ri, float r2f,
     return r2f * uf * uf <= rhs * rhs * 1.0001f;
 }
 
-__device__ __noinline__ u4 philox_accept(uint32_t blk, uint32_t i, uint32_t pid, uint32_t k0, uint32_t k1) {
+__device__ __forceinline__ u4 philox_accept(uint32_t blk, uint32_t i, uint32_t pid, uint32_t k0, uint32_t k1) {
     return philox(blk, i, pid, 3u, k0, k1);
 }
 
@@ -555,7 +555,10 @@ __device__ __forceinline__ uint32_t init_batch(const IrtConst& C, const InitTrac
     return np;
 }
 
-__global__ void __launch_bounds__(IB) k_irt_init(IArgs A) {
+#ifndef WG_INIT_MINB
+#define WG_INIT_MINB 6
+#endif
+__global__ void __launch_bounds__(IB, WG_INIT_MINB) k_irt_init(IArgs A) {
     __shared__ IrtConst s_c;
     __shared__ uint32_t s_row[6];
     __shared__ float4 s_pj[IB / 32][32];
@@ -595,38 +598,57 @@ __global__ void __launch_bounds__(IB) k_irt_init(IArgs A) {
         if (hi_) me = pf[i];
         const int si = hi_ ? __float_as_int(me.w) : 0;
         const uint32_t row = s_row[si];
-        uint32_t cblk = 0xffffffffu;
-        u4 cw = {0, 0, 0, 0};
         int qn = 0;
         for (uint32_t j0 = i0; j0 < n; j0 += 32) {
             __syncwarp();
             if (j0 + lane < n) s_pj[wl][lane] = pf[j0 + lane];
             __syncwarp();
             const uint32_t kmax = min(32u, n - j0);
-            for (uint32_t kk = 0; kk < kmax; ++kk) {
-                const uint32_t j = j0 + kk;
-                const float4 q = s_pj[wl][kk];
-                const int sj = __float_as_int(q.w);
-                const int ri = (int)((row >> (4 * sj)) & 15u);
-                int kind = 0;                           // 1: candidate, 2: near R_CUT
-                uint32_t wd = 0;
-                if (hi_ && j > i && ri != 15) {
-                    float dx = me.x - q.x, dy = me.y - q.y, dz = me.z - q.z;
-                    float r2f = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                    if (r2f < lo2) {
-                        n_pairs++;
-                        if ((j >> 2) != cblk) { cblk = j >> 2; cw = philox_accept(cblk, i, T.pid, A.k0, A.k1); }
-                        wd = (j & 3) == 0 ? cw.x : (j & 3) == 1 ? cw.y : (j & 3) == 2 ? cw.z : cw.w;
-                        if (pair_maybe(C, ri, r2f, del, wd)) kind = 1;
-                    } else if (r2f <= hi2) kind = 2;
+            // partners in groups of 4 = one Philox block of acceptance words
+            // (j0 is a multiple of 32): 4 distances, at most one Philox call
+            for (uint32_t kk = 0; kk < kmax; kk += 4) {
+                float r2[4];
+                int rr[4], sv[4];
+                bool ok[4];
+                bool need = false;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const uint32_t j = j0 + kk + u;
+                    const float4 q = s_pj[wl][kk + u];
+                    const bool in = kk + u < kmax;
+                    sv[u] = in ? __float_as_int(q.w) : 0;
+                    rr[u] = (int)((row >> (4 * sv[u])) & 15u);
+                    ok[u] = in && hi_ && j > i && rr[u] != 15;
+                    const float dx = me.x - q.x, dy = me.y - q.y, dz = me.z - q.z;
+                    r2[u] = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                    need |= ok[u] && r2[u] < lo2;
                 }
-                const unsigned m = __ballot_sync(FULL, kind != 0);
-                if (m) {
-                    if (kind) {
+                u4 cw = {0, 0, 0, 0};
+                if (need) cw = philox_accept((j0 + kk) >> 2, i, T.pid, A.k0, A.k1);
+                int kind[4];                            // 1: candidate, 2: near R_CUT
+                bool any = false;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const uint32_t wd = u == 0 ? cw.x : u == 1 ? cw.y : u == 2 ? cw.z : cw.w;
+                    kind[u] = 0;
+                    if (ok[u]) {
+                        if (r2[u] < lo2) {
+                            n_pairs++;
+                            if (pair_maybe(C, rr[u], r2[u], del, wd)) kind[u] = 1;
+                        } else if (r2[u] <= hi2) kind[u] = 2;
+                    }
+                    any |= kind[u] != 0;
+                }
+                if (!__any_sync(FULL, any)) continue;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const unsigned m = __ballot_sync(FULL, kind[u] != 0);
+                    if (!m) continue;
+                    if (kind[u]) {
                         const int at = qn + __popc(m & lt);
-                        qij[at] = (i << 16) | j;
-                        qw[at] = wd;
-                        qk[at] = (uint16_t)(kind | (ri << 2) | (si << 6) | (sj << 9));
+                        qij[at] = (i << 16) | (j0 + kk + u);
+                        qw[at] = u == 0 ? cw.x : u == 1 ? cw.y : u == 2 ? cw.z : cw.w;
+                        qk[at] = (uint16_t)(kind[u] | (rr[u] << 2) | (si << 6) | (sv[u] << 9));
                     }
                     qn += __popc(m);
                     if (qn >= 32) {
