@@ -673,10 +673,10 @@ __global__ void __launch_bounds__(IB, WG_INIT_MINB) k_irt_init(IArgs A) {
     if (lane == 0 && n_pairs) atomicAdd(&A.acc[10], n_pairs);
 }
 
-__device__ __noinline__ u4 philox_pair(uint32_t id, uint32_t jj, uint32_t pid, uint32_t k0, uint32_t k1) {
+__device__ __forceinline__ u4 philox_pair(uint32_t id, uint32_t jj, uint32_t pid, uint32_t k0, uint32_t k1) {
     return philox(id, jj, pid, 5u, k0, k1);
 }
-__device__ __noinline__ u4 philox_pair_ang(uint32_t id, uint32_t jj, uint32_t pid, uint32_t k0, uint32_t k1) {
+__device__ __forceinline__ u4 philox_pair_ang(uint32_t id, uint32_t jj, uint32_t pid, uint32_t k0, uint32_t k1) {
     return philox(id, jj, pid, 5u | (1u << 4), k0, k1);
 }
 
