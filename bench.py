@@ -43,9 +43,10 @@ WORKLOAD = ("4096 x 10 keV e- in liquid water, box +-15 um, cutoff 7.5 eV, Philo
             "IRT to 1 us -> direct SSB + DSB on 21x21 B-DNA fibres")
 CPU_SAMPLE_PRIMARIES = 512
 # library kernels per step: transport 1, rad_buf canonical order 5 (histogram,
-# scan, scatter, segment sort, reduce), IRT 6 (segment max, load, scan,
-# pairing, order, events), scoring 5 (prep, tiles, tile scan, apply, cluster)
-LAUNCHES_PER_STEP = 17
+# scan, scatter, segment sort, reduce), IRT 7 (segment max, load, scan,
+# pairing, order, initial-event sort, events), scoring 5 (prep, tiles, tile
+# scan, apply, cluster)
+LAUNCHES_PER_STEP = 18
 
 
 def peaks():
@@ -234,7 +235,7 @@ def run_native(args, ws, rank, local):
         torch.cuda.synchronize()
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    t_tr, t_irt, t_canon, t_sc, t_pair, t_evl = [], [], [], [], [], []
+    t_tr, t_irt, t_canon, t_sc, t_pair, t_evl, t_sort = [], [], [], [], [], [], []
     launches = 0
     with Clocks(local) as clk:
         barrier()
@@ -250,6 +251,7 @@ def run_native(args, ws, rank, local):
             t_irt.append(ir.ms)
             t_pair.append(ir.ms_pairing)
             t_evl.append(ir.ms_events)
+            t_sort.append(ir.ms_sort)
             t_sc.append(ssb.ms + dsb.ms)
             launches += LAUNCHES_PER_STEP
         barrier()
@@ -280,7 +282,8 @@ def run_native(args, ws, rank, local):
     pk = peaks()
     mean = lambda a: sum(a) / len(a)
     stages = {"irt": mean(t_irt), "transport": mean(t_tr), "canon": mean(t_canon), "scoring": mean(t_sc)}
-    kernels = {"k_transport": mean(t_tr), "k_irt_init": mean(t_pair), "k_irt_loop": mean(t_evl)}
+    kernels = {"k_transport": mean(t_tr), "k_irt_init": mean(t_pair), "k_irt_loop": mean(t_evl),
+               "k_track_order+k_irt_sort": mean(t_sort)}
     dom = max(kernels, key=kernels.get)
     R, S, D = st.rad_n_stored, st.sec_n, st.dbg[5]
     Np, Ei, Et = ir.n_particles, ir.n_init_events, ir.n_events

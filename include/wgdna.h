@@ -109,6 +109,7 @@ typedef struct {
     float ms;                   /* whole IRT on the device */
     float ms_load, ms_pairing, ms_events;   /* its kernels: load + displacement, initial pairing, event loop */
     uint32_t device_error;
+    float ms_sort;              /* ordering of the tracks and sort of their initial events (before the event loop) */
 } wgdna_irt_result;
 
 /* runChemistryWorker (src/chemistry/worker.ts:32-87, public/irt-worker.js:370-699)

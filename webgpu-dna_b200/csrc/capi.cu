@@ -108,7 +108,7 @@ struct wgdna_ctx {
     double* d_acc_tl = nullptr;
     unsigned long long* d_acc = nullptr;
     uint32_t* d_maxpid = nullptr;
-    cudaEvent_t ev[10]{};
+    cudaEvent_t ev[11]{};
 };
 
 static std::string lib_dir() {
@@ -486,7 +486,8 @@ static int irt_run(wgdna_ctx* c, uint32_t nseg, uint32_t n_therm, double E_eV, u
         cudaEventElapsedTime(&out->ms, c->ev[4], c->ev[5]);
         cudaEventElapsedTime(&out->ms_load, c->ev[4], c->ev[8]);
         cudaEventElapsedTime(&out->ms_pairing, c->ev[8], c->ev[9]);
-        cudaEventElapsedTime(&out->ms_events, c->ev[9], c->ev[5]);
+        cudaEventElapsedTime(&out->ms_sort, c->ev[9], c->ev[10]);
+        cudaEventElapsedTime(&out->ms_events, c->ev[10], c->ev[5]);
         out->device_error = err;
     }
     if (err) { wg_set_error("wgdna_irt: device error flags 0x%x", err); return WGDNA_ERR_DEVICE; }

@@ -299,29 +299,6 @@ __device__ void heap_pop(const Heap& H, uint32_t& n) {
     H.set(p, tp, ap);
 }
 
-// warp bitonic sort of n events (t, ab) in global memory, ascending
-__device__ void warp_sort(double* T, uint32_t* AB, uint32_t n, int lane) {
-    uint32_t n2 = 1;
-    while (n2 < n) n2 <<= 1;
-    for (uint32_t k = n + lane; k < n2; k += 32) { T[k] = 1e300; AB[k] = 0xffffffffu; }
-    __syncwarp();
-    for (uint32_t k = 2; k <= n2; k <<= 1) {
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = lane; i < n2; i += 32) {
-                uint32_t l = i ^ j;
-                if (l > i) {
-                    double ti = T[i], tl = T[l];
-                    uint32_t ai = AB[i], al = AB[l];
-                    bool up = (i & k) == 0;
-                    if (ev_less(tl, al, ti, ai) == up) { T[i] = tl; T[l] = ti; AB[i] = al; AB[l] = ai; }
-                }
-            }
-            __syncwarp();
-            __threadfence_block();
-        }
-    }
-}
-
 constexpr uint32_t FULL = 0xffffffffu;
 
 // Per-track storage (one track = one primary): particle slots at
@@ -763,7 +740,49 @@ __device__ __forceinline__ bool prod_batch(const IrtConst& C, const ProdCtx& P, 
     return __any_sync(FULL, over);
 }
 
-// 3) events (:566-660): sort the initial events, then pop in (t, i, j) order
+// 3a) the initial events of each track in (t, i, j) order (:566): a block-wide
+//     bitonic sort, in shared memory up to SORT_SM events (padded to a power
+//     of two), in the track's own event slots beyond that (they hold 2 ecap).
+//     Keys are unique, so the order is that of any other sort.
+constexpr int SB = 256;
+constexpr uint32_t SORT_SM = 4096;
+__global__ void __launch_bounds__(SB) k_irt_sort(IArgs A) {
+    __shared__ double st[SORT_SM];
+    __shared__ uint32_t sab[SORT_SM];
+    for (uint32_t k = blockIdx.x; k < A.nseg; k += gridDim.x) {
+        const uint32_t p = A.order[k];                 // largest tracks first
+        const uint32_t nev = A.tev[p];
+        if (nev < 2 || nev > ecap(A, p)) continue;     // the event kernel reports the overflow
+        double* T = A.ev_t + ebase(A, p);
+        uint32_t* AB = A.ev_ab + ebase(A, p);
+        uint32_t n2 = 2;
+        while (n2 < nev) n2 <<= 1;
+        const bool sm = n2 <= SORT_SM;
+        double* t = sm ? st : T;
+        uint32_t* ab = sm ? sab : AB;
+        __syncthreads();                               // the previous track is written back
+        for (uint32_t i = threadIdx.x; i < n2; i += SB) {
+            if (i >= nev) { t[i] = 1e300; ab[i] = 0xffffffffu; }
+            else if (sm) { st[i] = T[i]; sab[i] = AB[i]; }
+        }
+        __syncthreads();
+        for (uint32_t kk = 2; kk <= n2; kk <<= 1) {
+            for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+                for (uint32_t q = threadIdx.x; q < (n2 >> 1); q += SB) {
+                    const uint32_t i = ((q & ~(j - 1)) << 1) | (q & (j - 1)), l = i | j;   // bit j of i clear
+                    const double ti = t[i], tl = t[l];
+                    const uint32_t ai = ab[i], al = ab[l];
+                    if (ev_less(tl, al, ti, ai) == ((i & kk) == 0)) { t[i] = tl; t[l] = ti; ab[i] = al; ab[l] = ai; }
+                }
+                __syncthreads();
+            }
+        }
+        if (sm)
+            for (uint32_t i = threadIdx.x; i < nev; i += SB) { T[i] = st[i]; AB[i] = sab[i]; }
+    }
+}
+
+// 3) events (:566-660): pop the sorted initial events in (t, i, j) order
 //    merged with a heap of product events; one warp per track
 #ifndef WG_LOOP_MINB
 #define WG_LOOP_MINB 4
@@ -820,7 +839,6 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
         if (nev > ecap(A, p)) { if (lane == 0) atomicOr(A.err, DERR_HEAP); continue; }
         if (lane == 0) tally[11] += nev;
         __syncwarp();
-        warp_sort(ET, EAB, nev, lane);
         uint32_t ip = 0, hn = 0;
         uint32_t ntot = n;
         double h2c = (double)A.th2[p];
@@ -1125,6 +1143,12 @@ cudaError_t launch_irt(const IArgs& a, int device, cudaStream_t s, cudaEvent_t* 
     k_irt_init<<<blocks_for((const void*)k_irt_init, device), IB, 0, s>>>(a);
     if (ev) cudaEventRecord(ev[1], s);
     k_track_order<<<1, 1024, 0, s>>>(a.tn, a.nseg, a.order);
+    int sms = 0, per = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)k_irt_sort, SB, 0);
+    const unsigned long long sgrid = (unsigned long long)sms * (unsigned long long)(per > 0 ? per : 1);
+    k_irt_sort<<<(unsigned)(a.nseg < sgrid ? (a.nseg > 0 ? a.nseg : 1) : sgrid), SB, 0, s>>>(a);
+    if (ev) cudaEventRecord(ev[2], s);
     k_irt_loop<<<blocks_for((const void*)k_irt_loop, device), IB, 0, s>>>(a);
     return cudaGetLastError();
 }

@@ -64,7 +64,7 @@ class IrtResult(C.Structure):
                 ("n_events", C.c_uint64), ("n_particles", C.c_uint64), ("n_init_events", C.c_uint64),
                 ("chem_n", C.c_uint64), ("ms", C.c_float),
                 ("ms_load", C.c_float), ("ms_pairing", C.c_float), ("ms_events", C.c_float),
-                ("device_error", C.c_uint32)]
+                ("device_error", C.c_uint32), ("ms_sort", C.c_float)]
 
 
 class ChemGridResult(C.Structure):
