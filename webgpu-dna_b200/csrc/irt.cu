@@ -657,6 +657,10 @@ __device__ __forceinline__ u4 philox_pair_ang(uint32_t id, uint32_t jj, uint32_t
     return philox(id, jj, pid, 5u | (1u << 4), k0, k1);
 }
 
+__device__ __noinline__ double gauss_axis(uint32_t wa, uint32_t wb) {
+    return sqrt(-2 * log_(u01d32(wa) + 1e-30)) * cos_(6.2831853 * u01d32(wb));
+}
+
 // the product being re-paired (uniform over the warp)
 struct ProdCtx {
     const double *px, *py, *pz, *tb;
@@ -697,9 +701,9 @@ __device__ __forceinline__ bool prod_batch(const IrtConst& C, const ProdCtx& P, 
             if (dist - sig * B > R) need = false;
             if (need) {
                 u4 q1 = philox(P.id, jj, P.pid, 5u | (1u << 4), P.k0, P.k1);
-                double g0 = sqrt(-2 * log_(u01d32(q0.x) + 1e-30)) * cos_(6.2831853 * u01d32(q1.x));
-                double g1 = sqrt(-2 * log_(u01d32(q0.y) + 1e-30)) * cos_(6.2831853 * u01d32(q1.y));
-                double g2 = sqrt(-2 * log_(u01d32(q0.z) + 1e-30)) * cos_(6.2831853 * u01d32(q1.z));
+                double g0 = gauss_axis(q0.x, q1.x);
+                double g1 = gauss_axis(q0.y, q1.y);
+                double g2 = gauss_axis(q0.z, q1.z);
                 xj += g0 * sig; yj += g1 * sig; zj += g2 * sig;
             }
         }
