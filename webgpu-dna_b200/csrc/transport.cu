@@ -634,18 +634,20 @@ __device__ __forceinline__ void finish_primary(const TArgs& A, Blk& b, Particle&
 
 // one warp-iteration of a lane's electron.  Primaries and secondaries share
 // one fly + interact call site, so a warp holding both kinds runs the step
-// code once instead of once per kind.
+// code once instead of once per kind; the lanes of `act` (those that entered)
+// meet again before the interaction, so its branches run once per warp step.
 __device__ __forceinline__ void lane_step(const TArgs& A, Blk& b, Particle& q, Dep& dep,
-                                          unsigned long long& nsteps) {
+                                          unsigned long long& nsteps, unsigned act) {
     const float box = A.box;
     const bool prim = q.prim;
     const bool out = fabsf(q.px) >= box || fabsf(q.py) >= box || fabsf(q.pz) >= box;
+    bool go = true;
     if (prim) {
-        if (q.it >= A.ms || q.E < A.ce) { finish_primary(A, b, q, dep, 0u); return; }
-        if (out) { finish_primary(A, b, q, dep, 1u); return; }
+        if (q.it >= A.ms || q.E < A.ce) { finish_primary(A, b, q, dep, 0u); go = false; }
+        else if (out) { finish_primary(A, b, q, dep, 1u); go = false; }
     } else {
-        if (q.it >= A.sec_steps) { q.active = false; return; }
-        if (q.E < A.ce) {                                        // secondary.wgsl:100-124
+        if (q.it >= A.sec_steps) { q.active = false; go = false; }
+        else if (q.E < A.ce) {                                   // secondary.wgsl:100-124
             deposit(A, dep, q.px, q.py, q.pz, q.E);
             atomicAdd(&b.cnt[C_EAQ], 1u);
             float eaq_s = meesungnoen_sigma(q.E);
@@ -657,34 +659,40 @@ __device__ __forceinline__ void lane_step(const TArgs& A, Blk& b, Particle& q, D
             put(A, b, q, epx, epy, epz, 5.0f);
             atomicAdd(&b.cnt[SS_CUT], 1u);
             q.active = false;
-            return;
-        }
-        if (out) {
+            go = false;
+        } else if (out) {
             atomicAdd(&b.cnt[SS_BOUNDS], 1u);
             q.active = false;
-            return;
+            go = false;
         }
     }
-    const bool productive = q.E > 12.0f;
-    XS x; float dist;
-    if (!fly(A, b, q, x, dist)) {
-        if (prim) finish_primary(A, b, q, dep, 0u);
-        else q.active = false;
-        return;
+    XS x;
+    if (go) {
+        const bool productive = q.E > 12.0f;
+        float dist;
+        if (!fly(A, b, q, x, dist)) {
+            if (prim) finish_primary(A, b, q, dep, 0u);
+            else q.active = false;
+            go = false;
+        } else {
+            nsteps++;
+            if (prim) {
+                q.tpath += dist;
+                if (productive) q.ppath += dist;
+                float rdx = q.px - q.sx, rdy = q.py - q.sy, rdz = q.pz - q.sz;
+                float r = sqrtf(rdx * rdx + rdy * rdy + rdz * rdz);
+                if (r > q.maxr) q.maxr = r;
+                if (fabsf(q.px) >= box || fabsf(q.py) >= box || fabsf(q.pz) >= box) { finish_primary(A, b, q, dep, 1u); go = false; }
+            } else {
+                atomicAdd(&b.cnt[SS_STEPS], 1u);
+            }
+        }
     }
-    nsteps++;
-    if (prim) {
-        q.tpath += dist;
-        if (productive) q.ppath += dist;
-        float rdx = q.px - q.sx, rdy = q.py - q.sy, rdz = q.pz - q.sz;
-        float r = sqrtf(rdx * rdx + rdy * rdy + rdz * rdz);
-        if (r > q.maxr) q.maxr = r;
-        if (fabsf(q.px) >= box || fabsf(q.py) >= box || fabsf(q.pz) >= box) { finish_primary(A, b, q, dep, 1u); return; }
-    } else {
-        atomicAdd(&b.cnt[SS_STEPS], 1u);
+    __syncwarp(act);
+    if (go) {
+        interact(A, b, q, dep, x);
+        q.it++;
     }
-    interact(A, b, q, dep, x);
-    q.it++;
 }
 
 __device__ __forceinline__ void flush_staging(const TArgs& A, Blk& b, int lane) {
@@ -826,7 +834,7 @@ __global__ void __launch_bounds__(TB, 2) k_transport(TArgs A) {
         }
         sleep_ns = 64;
         idle_since = 0;
-        if (q.active) lane_step(A, b, q, dep, nsteps);
+        if (q.active) lane_step(A, b, q, dep, nsteps, act);
         __syncwarp();
         // stash overflow went straight to the global queue; spill a full stash
         if (lane == 0) {
