@@ -469,6 +469,34 @@ def run_mixed(args):
     nth = int((o["results"].view(np.uint32).reshape(-1, 8)[:, 5] == 0).sum())
     oracle.irt(o["rad"], nth, Emean, seed=7, nthreads=nthreads)
     cpu = sample / (time.perf_counter() - t0)
+    # per species-count bucket: the IRT alone on the tracks of that bucket (host rad_buf
+    # of the same transport, re-run through wgdna_run_irt); results per track do not
+    # depend on which other tracks share the launch
+    rad = np.empty(st.rad_n_stored * 4, np.float32)
+    rn = C.c_uint64()
+    _lib.check("wgdna_transport_copy_out", L.wgdna_transport_copy_out(ctx.h, None, None, _lib.ptr(rad),
+                                                                      st.rad_n_stored, C.byref(rn)))
+    rad = rad[:4 * min(rn.value, st.rad_n_stored)].reshape(-1, 4)
+    w = rad[:, 3].astype(np.int64)
+    pid, code = w >> 3, w & 7
+    tracked = np.bincount(pid[code != 7], minlength=N)
+    buckets = []
+    edges = (1, 100, 500, 1000, 2000, 5000, 1 << 30)
+    irb = _lib.IrtResult()
+    for lo, hi in zip(edges[:-1], edges[1:]):
+        sel = np.nonzero((tracked >= lo) & (tracked < hi))[0]
+        if sel.size == 0:
+            continue
+        sub = np.ascontiguousarray(rad[np.isin(pid, sel)])
+        ms = []
+        for k in range(3):
+            _lib.check("wgdna_run_irt", L.wgdna_run_irt(ctx.h, _lib.ptr(sub), sub.shape[0], int(sel.size), Emean,
+                                                        args.seed + 1, C.byref(irb)))
+            ms.append(irb.ms)
+        ms = sorted(ms)[1]
+        buckets.append({"species": f"{lo}-{hi - 1}" if hi < (1 << 30) else f">={lo}", "tracks": int(sel.size),
+                        "irt_species": int(irb.n_particles), "pairs": int(irb.n_pairs), "events": int(irb.n_events),
+                        "irt_ms": round(ms, 3), "pairs_per_s": irb.n_pairs / (ms / 1000.0)})
     line = {"metric": "mixed-energy primaries/s (transport+IRT)", "value": value, "unit": "primaries/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 transport / f64 IRT",
@@ -483,6 +511,7 @@ def run_mixed(args):
             "clocks": clk.summary(),
             "work": {"rad_n": int(R), "sec_n": int(S), "tracks": int(ir.n_tracks), "irt_species": int(ir.n_particles),
                      "irt_pairs": int(ir.n_pairs), "irt_events": int(ir.n_events)},
+            "irt_buckets": buckets,
             "cpu_baseline": {"value": cpu, "unit": "primaries/s", "cores": nthreads, "kind": "port",
                              "sample": f"first {sample} primaries of the same energy list, oracle transport + IRT"}}
     print(json.dumps(line), flush=True)
