@@ -853,11 +853,13 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
         for (;;) {
             double et = 0;
             uint32_t eab = 0;
-            int have = 0;
+            int have = 0, si = 0, sj = 0, ri = -1;
             if (lane == 0) {
-                bool hi_ = ip < nev, hh = hn > 0;
-                if (hi_ || hh) {
-                    have = 1;
+                // pop until a reaction with products: stale events and reactions
+                // without products change nothing the other lanes work on
+                for (;;) {
+                    const bool hi_ = ip < nev, hh = hn > 0;
+                    if (!hi_ && !hh) break;
                     double ti = hi_ ? ET[ip] : 0.0, th = hh ? H.t(0) : 0.0;
                     uint32_t ai = hi_ ? EAB[ip] : 0u, ah = hh ? H.ab(0) : 0u;
                     if (hi_ && (!hh || ev_less(ti, ai, th, ah))) { et = ti; eab = ai; ip++; }
@@ -875,42 +877,37 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
                         c[4] = (float)h2c;
                         c16++;
                     }
+                    const int ei = (int)(eab >> 16), ej = (int)(eab & 0xffffu);
+                    if (!(alive[ei] && alive[ej])) continue;
+                    const int a = sp[ei], b2 = sp[ej];
+                    const int r = C.map[(a < b2 ? a : b2) * 6 + (a < b2 ? b2 : a)];
+                    if (r < 0) continue;
+                    alive[ei] = 0; alive[ej] = 0;
+                    for (int w2 = 0; w2 < 2; ++w2) {
+                        int k = w2 == 0 ? ei : ej, q = w2 == 0 ? a : b2;
+                        uint32_t at = lpos[k];
+                        uint16_t last = lst[q * cap + lc[q] - 1];
+                        lst[q * cap + at] = last;
+                        rec[q * cap + at] = rec[q * cap + lc[q] - 1];
+                        lpos[last] = (uint16_t)at;
+                        lc[q]--;
+                    }
+                    tally[9]++;
+                    tally[r]++;
+                    if (r == 3 || r == 4 || r == 6) h2c += 1;
+                    if (C.nprod[r] == 0) continue;
+                    have = 1; si = a; sj = b2; ri = r;
+                    break;
                 }
             }
             if (!__shfl_sync(FULL, have, 0)) break;
             et = __shfl_sync(FULL, et, 0);
             eab = __shfl_sync(FULL, eab, 0);
-            int ei = (int)(eab >> 16), ej = (int)(eab & 0xffffu);
-            int valid = 0, si = 0, sj = 0, ri = -1;
-            if (lane == 0) {
-                if (alive[ei] && alive[ej]) {
-                    si = sp[ei]; sj = sp[ej];
-                    ri = C.map[(si < sj ? si : sj) * 6 + (si < sj ? sj : si)];
-                    if (ri >= 0) {
-                        valid = 1;
-                        alive[ei] = 0; alive[ej] = 0;
-                        for (int w2 = 0; w2 < 2; ++w2) {
-                            int k = w2 == 0 ? ei : ej, q = w2 == 0 ? si : sj;
-                            uint32_t at = lpos[k];
-                            uint16_t last = lst[q * cap + lc[q] - 1];
-                            lst[q * cap + at] = last;
-                            rec[q * cap + at] = rec[q * cap + lc[q] - 1];
-                            lpos[last] = (uint16_t)at;
-                            lc[q]--;
-                        }
-                        tally[9]++;
-                        tally[ri]++;
-                        if (ri == 3 || ri == 4 || ri == 6) h2c += 1;
-                    }
-                }
-            }
-            valid = __shfl_sync(FULL, valid, 0);
-            if (!valid) continue;
+            const int ei = (int)(eab >> 16), ej = (int)(eab & 0xffffu);
             si = __shfl_sync(FULL, si, 0);
             sj = __shfl_sync(FULL, sj, 0);
             ri = __shfl_sync(FULL, ri, 0);
-            int np_ = C.nprod[ri];
-            if (np_ == 0) continue;
+            const int np_ = C.nprod[ri];
             double sqDi = sqrt(C.D[si]), sqDj = sqrt(C.D[sj]);
             double ww = sqDi + sqDj;
             double xa = px[ei], ya = py[ei], za = pz[ei];
