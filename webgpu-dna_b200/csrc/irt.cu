@@ -952,20 +952,21 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
                     const float fs = C.fs[r2i], fsc = C.fsc[r2i], fadd = C.fadd[r2i];
                     const uint16_t* L2 = lst + s2 * cap;
                     const float4* R2 = rec + s2 * cap;
-                    // PU chunks of 32 partners at a time: independent loads and Philox blocks
-                    for (uint32_t c0 = 0; c0 < len; c0 += 32 * PU) {
+                    // chunks of 32 partners; the next chunk's list entry and record are
+                    // loaded before this chunk is tested (the lists do not change here)
+                    static_assert(PU == 1, "one chunk at a time");
+                    uint32_t jnext = lane < len ? L2[lane] : 0xffffu;
+                    float4 rnext = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (lane < len) rnext = R2[lane];
+                    for (uint32_t c0 = 0; c0 < len; c0 += 32) {
                         uint32_t jv[PU];
                         bool mv[PU];
-#pragma unroll
-                        for (int u = 0; u < PU; ++u) {
-                            const uint32_t li = c0 + 32u * u + lane;
-                            jv[u] = li < len ? L2[li] : 0xffffu;
-                        }
                         float4 qv[PU];
-#pragma unroll
-                        for (int u = 0; u < PU; ++u) {
-                            const uint32_t li = c0 + 32u * u + lane;
-                            if (li < len) qv[u] = R2[li];
+                        jv[0] = jnext; qv[0] = rnext;
+                        {
+                            const uint32_t li = c0 + 32u + lane;
+                            jnext = li < len ? L2[li] : 0xffffu;
+                            if (li < len) rnext = R2[li];
                         }
 #pragma unroll
                         for (int u = 0; u < PU; ++u) {
