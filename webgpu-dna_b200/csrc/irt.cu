@@ -12,8 +12,11 @@
 // * initial pairing: tiles of 32 particles held in lane registers, the partner
 //   j broadcast to all lanes; one Philox block gives the acceptance draws of
 //   four consecutive partners;
-// * events: a binary heap ordered by (t, i, j), kept by lane 0; the
-//   product re-pairing (pairWithAlive) is spread over the 32 lanes.
+// * sort: the initial events of a track in (t, i, j) order, one block per
+//   track, in shared memory;
+// * events: the sorted initial events merged with a binary heap of product
+//   events ordered by (t, i, j), kept by lane 0; the product re-pairing
+//   (pairWithAlive) is spread over the 32 lanes.
 //
 // Random draws are keyed by what they are for (track, particle, pair), so the
 // result does not depend on scheduling; the CPU oracle uses the same streams:
@@ -744,7 +747,7 @@ __device__ __forceinline__ bool prod_batch(const IrtConst& C, const ProdCtx& P, 
     return __any_sync(FULL, over);
 }
 
-// 3a) the initial events of each track in (t, i, j) order (:566): a block-wide
+// 3) the initial events of each track in (t, i, j) order (:566): a block-wide
 //     bitonic sort, in shared memory up to SORT_SM events (padded to a power
 //     of two), in the track's own event slots beyond that (they hold 2 ecap).
 //     Keys are unique, so the order is that of any other sort.
@@ -786,7 +789,7 @@ __global__ void __launch_bounds__(SB) k_irt_sort(IArgs A) {
     }
 }
 
-// 3) events (:566-660): pop the sorted initial events in (t, i, j) order
+// 4) events (:566-660): pop the sorted initial events in (t, i, j) order
 //    merged with a heap of product events; one warp per track
 #ifndef WG_LOOP_MINB
 #define WG_LOOP_MINB 4
