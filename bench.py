@@ -284,7 +284,7 @@ def run_native(args, ws, rank, local):
     stages = {"irt": mean(t_irt), "transport": mean(t_tr), "canon": mean(t_canon), "scoring": mean(t_sc)}
     kernels = {"k_transport": mean(t_tr), "k_irt_init": mean(t_pair), "k_irt_loop": mean(t_evl),
                "k_track_order+k_irt_sort": mean(t_sort)}
-    dom = max(kernels, key=kernels.get)
+    dom = max(("k_transport", "k_irt_init", "k_irt_loop"), key=kernels.get)
     R, S, D = st.rad_n_stored, st.sec_n, st.dbg[5]
     Np, Ei, Et = ir.n_particles, ir.n_init_events, ir.n_events
     alg = {
