@@ -664,10 +664,11 @@ __device__ __noinline__ double gauss_axis(uint32_t wa, uint32_t wb) {
     return sqrt(-2 * log_(u01d32(wa) + 1e-30)) * cos_(6.2831853 * u01d32(wb));
 }
 
-// the product being re-paired (uniform over the warp)
+// the product being re-paired (uniform over the warp); its position and
+// birth time are read back from its slot when a batch needs them
 struct ProdCtx {
     const double *px, *py, *pz, *tb;
-    double nx, ny, nz, et, Di;
+    double Di;
     uint32_t id, pid, k0, k1;
 };
 
@@ -681,12 +682,13 @@ __device__ __forceinline__ bool prod_batch(const IrtConst& C, const ProdCtx& P, 
     bool acc = false, pdcq = false, over = false;
     double ta = 0, pa = 0, pb = 0, pD = 0;
     uint32_t jj = 0;
+    const double pnx = P.px[P.id], pny = P.py[P.id], pnz = P.pz[P.id], pet = P.tb[P.id];
     if (lane < cnt) {
         const uint32_t e = pq[lane];
         jj = e & 0xffffu;
         const int r2i = (int)((e >> 16) & 15u), s2 = (int)(e >> 20);
         const double Dj = C.D[s2];
-        const double dt = P.et - P.tb[jj];
+        const double dt = pet - P.tb[jj];
         double xj = P.px[jj], yj = P.py[jj], zj = P.pz[jj];
         const u4 q0 = philox(P.id, jj, P.pid, 5u, P.k0, P.k1);
         const double U = u01d32(q0.w);
@@ -699,7 +701,7 @@ __device__ __forceinline__ bool prod_batch(const IrtConst& C, const ProdCtx& P, 
             float l1 = -2.0f * __logf((float)u01d32(q0.y));
             float l2 = -2.0f * __logf((float)u01d32(q0.z));
             double B = (double)sqrtf((l0 + l1 + l2) * 1.0001f) + 1e-4;
-            double ex = P.nx - xj, ey = P.ny - yj, ez = P.nz - zj;
+            double ex = pnx - xj, ey = pny - yj, ez = pnz - zj;
             double dist = sqrt(ex * ex + ey * ey + ez * ez);
             if (dist - sig * B > R) need = false;
             if (need) {
@@ -711,13 +713,13 @@ __device__ __forceinline__ bool prod_batch(const IrtConst& C, const ProdCtx& P, 
             }
         }
         if (need) {
-            double dx = P.nx - xj, dy = P.ny - yj, dz = P.nz - zj;
+            double dx = pnx - xj, dy = pny - yj, dz = pnz - zj;
             double r2 = dx * dx + dy * dy + dz * dz;
             if (r2 <= C.r_cut2) {
                 double D = P.Di + Dj;
                 double t = sample_pre(C, sqrt(r2), r2i, D, U, &pa, &pb);
                 if (t == -2.0) { pdcq = true; pD = D; }
-                else if (t >= 0) { ta = P.et + t; acc = ta < 1000; }
+                else if (t >= 0) { ta = pet + t; acc = ta < 1000; }
             }
         }
     }
@@ -728,7 +730,7 @@ __device__ __forceinline__ bool prod_batch(const IrtConst& C, const ProdCtx& P, 
         uint32_t qj = __shfl_sync(FULL, jj, src);
         double qa = __shfl_sync(FULL, pa, src), qb = __shfl_sync(FULL, pb, src);
         double X = pdc_warp(P.id, qj, P.pid, P.k0, P.k1, qa, qb, lane);
-        if (lane == src && X > 0) { ta = P.et + X / pD; acc = ta < 1000; }
+        if (lane == src && X > 0) { ta = pet + X / pD; acc = ta < 1000; }
     }
     unsigned m = __ballot_sync(FULL, acc);
     while (m) {
@@ -911,22 +913,24 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
             sj = __shfl_sync(FULL, sj, 0);
             ri = __shfl_sync(FULL, ri, 0);
             const int np_ = C.nprod[ri];
-            double sqDi = sqrt(C.D[si]), sqDj = sqrt(C.D[sj]);
-            double ww = sqDi + sqDj;
-            double xa = px[ei], ya = py[ei], za = pz[ei];
-            double xb = px[ej], yb = py[ej], zb = pz[ej];
-            double mx = (sqDj * xa + sqDi * xb) / ww;
-            double my = (sqDj * ya + sqDi * yb) / ww;
-            double mz = (sqDj * za + sqDi * zb) / ww;
             for (int pp = 0; pp < np_; ++pp) {
                 int nsp = pp == 0 ? C.prod0[ri] : C.prod1[ri];
                 uint32_t id = ntot;
                 if (id >= capref) break;                 // the reference's CAP (:405, :621)
                 if (id >= cap) { if (lane == 0) atomicOr(A.err, DERR_TRACK_SIZE); break; }
                 double nx, ny, nz;
-                if (np_ == 1) { nx = mx; ny = my; nz = mz; }
-                else if (pp == 0) { nx = xa; ny = ya; nz = za; }
-                else { nx = xb; ny = yb; nz = zb; }
+                if (np_ == 1) {                          // at the diffusion-weighted centre
+                    const double sqDi = sqrt(C.D[si]), sqDj = sqrt(C.D[sj]);
+                    const double ww = sqDi + sqDj;
+                    const double xa = px[ei], ya = py[ei], za = pz[ei];
+                    const double xb = px[ej], yb = py[ej], zb = pz[ej];
+                    nx = (sqDj * xa + sqDi * xb) / ww;
+                    ny = (sqDj * ya + sqDi * yb) / ww;
+                    nz = (sqDj * za + sqDi * zb) / ww;
+                } else {                                 // at the two reactants
+                    const int e = pp == 0 ? ei : ej;
+                    nx = px[e]; ny = py[e]; nz = pz[e];
+                }
                 const float nsx = (float)(nx - ox), nsy = (float)(ny - oy), nsz = (float)(nz - oz);
                 if (lane == 0) {
                     px[id] = nx; py[id] = ny; pz[id] = nz; tb[id] = et;
@@ -945,7 +949,7 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
                 const double Di = C.D[nsp];
                 const uint32_t rowp = s_row[nsp];
                 int qn = 0;
-                const ProdCtx P{px, py, pz, tb, nx, ny, nz, et, Di, id, pid, A.k0, A.k1};
+                const ProdCtx P{px, py, pz, tb, Di, id, pid, A.k0, A.k1};
                 const float etf = (float)et, dtm = 1e-4f + 1e-6f * etf;
                 for (int s2 = 0; s2 < 6; ++s2) {
                     const int r2i = (int)((rowp >> (4 * s2)) & 15u);
