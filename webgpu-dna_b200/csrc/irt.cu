@@ -303,6 +303,8 @@ __device__ void heap_pop(const Heap& H, uint32_t& n) {
 }
 
 constexpr uint32_t FULL = 0xffffffffu;
+// checkpoint times of the reference timeline (:566-580), ns
+__constant__ double c_cp[7] = {0.001, 0.01, 0.1, 1, 10, 100, 1000};
 
 // Per-track storage (one track = one primary): particle slots at
 // tbase(p) = 2*seg_off[p] + 64*p with capacity 2*len + 64 (len = the track's
@@ -838,13 +840,10 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
         double* ET = A.ev_t + ebase(A, p);
         uint32_t* EAB = A.ev_ab + ebase(A, p);
         const uint32_t nev = A.tev[p];
-        float4* pf = A.pf + tb0;
         const float del = A.tdel[p];
         const float4 org = A.rad[A.seg_off[p]];
         const double ox = org.x, oy = org.y, oz = org.z;
         if (lane < 6) lc[lane] = (int)A.tlc[6 * p + lane];     // alive species of each kind
-        uint32_t n2 = 1;
-        while (n2 < nev) n2 <<= 1;
         if (nev > ecap(A, p)) { if (lane == 0) atomicOr(A.err, DERR_HEAP); continue; }
         if (lane == 0) tally[11] += nev;
         __syncwarp();
@@ -854,7 +853,6 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
         int cp = 0, c16 = 0;
         float* curve = A.curves ? A.curves + 80ull * p : nullptr;
         bool heap_over = false;
-        const double CP[7] = {0.001, 0.01, 0.1, 1, 10, 100, 1000};
         for (;;) {
             double et = 0;
             uint32_t eab = 0;
@@ -870,7 +868,7 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
                     if (hi_ && (!hh || ev_less(ti, ai, th, ah))) { et = ti; eab = ai; ip++; }
                     else { et = th; eab = ah; heap_pop(H, hn); }
                     tally[10]++;
-                    while (cp < 7 && et >= CP[cp]) {
+                    while (cp < 7 && et >= c_cp[cp]) {
                         s_tl[wl][cp * 5 + 0] += lc[0]; s_tl[wl][cp * 5 + 1] += lc[1];
                         s_tl[wl][cp * 5 + 2] += lc[2]; s_tl[wl][cp * 5 + 3] += lc[4];
                         s_tl[wl][cp * 5 + 4] += h2c;
