@@ -58,6 +58,8 @@ def test_irt_synthetic_track_bit_exact(ctx):
     _lib.check("wgdna_run_irt", _lib.lib().wgdna_run_irt(ctx.h, _lib.ptr(rad), rad.shape[0], 1, 10000.0, 1,
                                                          C.byref(r)))
     assert r.device_error == 0 and r.n_tracks == 1
+    # more initial events than the sort keeps in shared memory: the device-memory sort runs
+    assert r.n_init_events > 4096
     np.testing.assert_array_equal(np.array(r.counts), ref["tl"])
     np.testing.assert_array_equal(np.array(r.rxn_counts[:]), ref["rxn_counts"])
     assert (r.n_reacted, r.n_pairs, r.n_events) == (ref["n_reacted"], ref["n_pairs"], ref["n_events"])
