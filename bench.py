@@ -695,12 +695,14 @@ def main():
     if args.workload != "pipeline":
         {"track": run_track, "mixed": run_mixed, "surrogate": run_surrogate, "sweep": run_sweep}[args.workload](args)
         return
+    if args.impl == "reference":
+        # host cores only: no device and no process group; under torchrun rank 0
+        # alone measures and prints, the other ranks exit at once
+        run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
+        return
     ws, rank, local = dist_init(args)
     try:
-        if args.impl == "reference":
-            run_reference(args, ws, rank)
-        else:
-            run_native(args, ws, rank, local)
+        run_native(args, ws, rank, local)
     finally:
         if ws > 1:
             import torch.distributed as dist
