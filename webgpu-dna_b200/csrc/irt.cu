@@ -464,10 +464,6 @@ __device__ __forceinline__ u4 philox_accept(uint32_t blk, uint32_t i, uint32_t p
 //    every pair; the rare candidates (and pairs within rounding of R_CUT) are
 //    queued per warp and redone exactly in f64, 32 at a time, one per lane.
 constexpr int IQ = 64;                   // candidate queue per warp
-#ifndef WG_IRT_PU
-#define WG_IRT_PU 1
-#endif
-constexpr int PU = WG_IRT_PU;            // partner chunks per step of the product re-pairing
 
 struct InitTrack {
     const double *px, *py, *pz;
@@ -959,28 +955,22 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
                     const float4* R2 = rec + s2 * cap;
                     // chunks of 32 partners; the next chunk's list entry and record are
                     // loaded before this chunk is tested (the lists do not change here)
-                    static_assert(PU == 1, "one chunk at a time");
                     uint32_t jnext = lane < len ? L2[lane] : 0xffffu;
                     float4 rnext = make_float4(0.f, 0.f, 0.f, 0.f);
                     if (lane < len) rnext = R2[lane];
                     for (uint32_t c0 = 0; c0 < len; c0 += 32) {
-                        uint32_t jv[PU];
-                        bool mv[PU];
-                        float4 qv[PU];
-                        jv[0] = jnext; qv[0] = rnext;
+                        const uint32_t jj = jnext;
+                        const float4 q = rnext;
                         {
                             const uint32_t li = c0 + 32u + lane;
                             jnext = li < len ? L2[li] : 0xffffu;
                             if (li < len) rnext = R2[li];
                         }
-#pragma unroll
-                        for (int u = 0; u < PU; ++u) {
-                            const uint32_t jj = jv[u];
-                            mv[u] = false;
+                        bool mv = false;
+                        {
                             if (jj != 0xffffu && jj != id) {
                                 n_pairs++;
-                                const float4 q = qv[u];
-                                const u4 q0 = PU == 1 ? philox_pair(id, jj, pid, A.k0, A.k1) : philox(id, jj, pid, 5u, A.k0, A.k1);
+                                const u4 q0 = philox_pair(id, jj, pid, A.k0, A.k1);
                                 const float ex = nsx - q.x, ey = nsy - q.y, ez = nsz - q.z;
                                 const float dlo = (sqrtf(fmaf(ez, ez, fmaf(ey, ey, ex * ex))) - del) * 0.999998f;
                                 // R of r_acc for U >= uf, rounded up
@@ -996,8 +986,8 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
                                     Bf = sqrtf((l0 + l1 + l2) * 1.0001f);
                                     reach = sqrtf(Djf2 * dth) * 1.00001f * (Bf + 1e-4f);
                                 }
-                                mv[u] = !(dlo - reach > rhi);
-                                if (mv[u] && dth > 0.0f) {
+                                mv = !(dlo - reach > rhi);
+                                if (mv && dth > 0.0f) {
                                     // second stage: the partner displaced by the same Box-Muller draws in
                                     // f32.  Per axis |g_f - g| <= 2e-3 + 2e-5 |g| (sqrt of the log near 0,
                                     // fast log and cos, 2 ulp each), sigma within [sl, sh].
@@ -1013,15 +1003,14 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
                                     const float d2 = sqrtf(fmaf(fz, fz, fmaf(fy, fy, fx * fx)));
                                     const float eg = 2e-3f + 2e-5f * Bm;
                                     const float err = 1.7320508f * (sh * eg + 0.5f * (Bm + eg) * (sh - sl)) + del;
-                                    mv[u] = !((d2 - err) * 0.99999f > rhi);
+                                    mv = !((d2 - err) * 0.99999f > rhi);
                                 }
                             }
                         }
-#pragma unroll
-                        for (int u = 0; u < PU; ++u) {
-                            const unsigned m = __ballot_sync(FULL, mv[u]);
+                        {
+                            const unsigned m = __ballot_sync(FULL, mv);
                             if (m) {
-                                if (mv[u]) pq[qn + __popc(m & ((1u << lane) - 1u))] = jv[u] | ((uint32_t)r2i << 16) | ((uint32_t)s2 << 20);
+                                if (mv) pq[qn + __popc(m & ((1u << lane) - 1u))] = jj | ((uint32_t)r2i << 16) | ((uint32_t)s2 << 20);
                                 qn += __popc(m);
                                 if (qn >= 32) {
                                     __syncwarp();
