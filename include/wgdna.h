@@ -269,8 +269,7 @@ int wgdna_cluster_device(wgdna_ctx *ctx, wgdna_dsb_result *dsb);
 
 /* Direct SSB scoring that allocates nothing.  No counterpart in the reference:
  * it serves callers that cannot call cudaMalloc (a host running under another
- * framework's memory pool or a fixed device-memory budget, or code that must
- * not allocate while a CUDA graph is being captured).  All pointers except
+ * framework's memory pool or a fixed device-memory budget).  All pointers except
  * `dna` and `out` are device pointers owned by the caller: d_rad holds rad_n
  * entries (16-byte aligned), d_fy/d_fz/d_rbb0/d_rbb1 the target built by
  * wgdna_build_dna_target, and d_hits (4-byte aligned, 2*n_bp bytes rounded up

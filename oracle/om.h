@@ -18,6 +18,13 @@
  *   sin/cos : reduction by multiples of pi/2 (three-part Cody-Waite constant),
  *          Taylor series of sin and cos on [-pi/4, pi/4], quadrant selection.
  *
+ * Split constants (the head has trailing zero bits so that k * head is exact):
+ * f32 ln2 0x3f317200 + 0x35bfbe8e as in fdlibm e_expf.c (Sun, 1993); f64 ln2
+ * 0x1.62e42fefa3800p-1 + 0x1.ef35793c76730p-45 as in ARM optimized-routines
+ * log_data.c; f32 pi/2 = twice DP1..DP3 of Cephes sinf.c (Moshier); f64 pi/2 =
+ * pio2_1..pio2_3 of fdlibm e_rem_pio2.c.  Error bounds in ulps are tested in
+ * tests/test_elementary.py through orc_elem (elem.c).
+ *
  * Every multiply-add that is fused is written as an explicit fmaf()/fma();
  * the file must be compiled with -ffp-contract=off so that nothing else is
  * fused.  The series coefficients are the exact rationals 1/n! and 1/(2k+1)

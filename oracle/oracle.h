@@ -119,6 +119,9 @@ void orc_dose_projection(const uint32_t *dose, uint32_t vc, int axis, float *pro
  * 7 checkpoints */
 int orc_chem_grid(const float *rad, uint32_t n, uint64_t seed, float *pos, uint32_t *alive, uint32_t counts[8][5]);
 
+/* elem.c: the elementary functions of om.h over a vector (fn codes in elem.c) */
+int orc_elem(int fn, const double *x, double *y, uint64_t n);
+
 #ifdef __cplusplus
 }
 #endif

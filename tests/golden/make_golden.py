@@ -9,7 +9,7 @@ Sources (paths inside the reference checkout):
                                                           summary.perEnergyHeadline: IRT G(1 us) at 1..20 keV
   tests/fixtures/geant4-reference.json                    Geant4-DNA 10 keV figures the reference compares to
 
-Usage:  python make_golden.py [reference checkout]   (default /root/reference)
+Usage:  python make_golden.py <reference checkout>   (or set WGDNA_REFERENCE)
 """
 import json
 import os
@@ -49,4 +49,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("WGDNA_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py <reference checkout> (or set WGDNA_REFERENCE)")
+    main(ref)

@@ -58,7 +58,8 @@ def _wgsl_source():
     return gen_tables.DEFAULT_SRC
 
 
-@pytest.mark.skipif(not os.path.exists(_wgsl_source()), reason="reference checkout not mounted")
+@pytest.mark.skipif(not (_wgsl_source() and os.path.exists(_wgsl_source())),
+                    reason="reference checkout not given (WGDNA_REFERENCE)")
 def test_blob_regenerates_bit_identical(tmp_path):
     """Re-parse the reference's WGSL and compare every array bit for bit."""
     import gen_tables

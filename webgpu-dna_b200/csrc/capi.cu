@@ -422,13 +422,14 @@ static int irt_ensure(wgdna_ctx* c, uint32_t nseg, uint64_t rad_n, uint32_t cap)
     if (!c->d_irt_cnt) TRY(dalloc(&c->d_irt_cnt, 4));
     if (!c->d_acc_tl) TRY(dalloc(&c->d_acc_tl, 35));
     if (!c->d_acc) TRY(dalloc(&c->d_acc, 16));
-    static bool consts = false;
-    if (!consts) {
+    // the reaction constants live in __constant__ memory, which every device
+    // holds separately: upload them once per device (the context's is current)
+    static DeviceOnce consts;
+    WG_CUDA_OK(consts.run([] {
         IrtConst C;
         irt_constants(&C);
-        WG_CUDA_OK(irt_set_constants(C));
-        consts = true;
-    }
+        return irt_set_constants(C);
+    }));
     return WGDNA_OK;
 }
 

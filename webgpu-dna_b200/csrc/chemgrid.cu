@@ -212,8 +212,8 @@ cudaError_t cg_run(const CgArgs& a, cudaStream_t s, cudaGraphExec_t* cache, CgGr
     const unsigned nb = (n + 255) / 256;
     cudaError_t e;
     k_cg_init<<<nb, 256, 0, s>>>(a.rad, n, a.k0, a.k1, a.pos, a.alive);
-    cudaMemsetAsync(a.counts, 0, 8 * 5 * sizeof(uint32_t), s);
-    cudaMemsetAsync(a.prod, 0, 2 * sizeof(uint32_t), s);
+    { cudaError_t me_ = cudaMemsetAsync(a.counts, 0, 8 * 5 * sizeof(uint32_t), s); if (me_ != cudaSuccess) return me_; }
+    { cudaError_t me_ = cudaMemsetAsync(a.prod, 0, 2 * sizeof(uint32_t), s); if (me_ != cudaSuccess) return me_; }
     k_cg_count<<<296, 256, 0, s>>>(a.pos, a.alive, n, a.prod, a.counts);
     // the schedule as one graph; rebuilt when the buffers or sizes change
     const CgGraphKey want{a.pos, a.alive, a.head, a.next, a.prod, a.counts, a.st, n, a.k0, a.k1};

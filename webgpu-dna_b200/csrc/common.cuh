@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 
 #include "../../include/wgdna.h"
 
@@ -79,6 +80,25 @@ struct __align__(16) SecRec {
 
 // A secondary waiting in a warp's shared-memory stash.
 struct StashRec { float x, y, z, E, dx, dy, dz; uint32_t pid, sub; };
+
+// Set-up that must happen once on every device that runs a kernel (constant
+// memory, function attributes): run(f) calls f with the current device when it
+// has not yet succeeded on that device.  Thread-safe; a failed f is retried.
+struct DeviceOnce {
+    std::mutex mu;
+    unsigned long long done[4] = {0, 0, 0, 0};   // device ordinals 0..255
+    template <class F> cudaError_t run(F f) {
+        int d = 0;
+        cudaError_t e = cudaGetDevice(&d);
+        if (e != cudaSuccess) return e;
+        if (d < 0 || d >= 256) return f();
+        std::lock_guard<std::mutex> lk(mu);
+        if ((done[d >> 6] >> (d & 63)) & 1ull) return cudaSuccess;
+        e = f();
+        if (e == cudaSuccess) done[d >> 6] |= 1ull << (d & 63);
+        return e;
+    }
+};
 
 }  // namespace wg
 

@@ -95,7 +95,7 @@ __global__ void k_expected_dsb(DoseDna d, const float* lambda, const uint8_t* hi
 }
 
 cudaError_t launch_dose_sum(const uint32_t* dose, uint64_t n, unsigned long long* out, cudaStream_t s) {
-    cudaMemsetAsync(out, 0, 8, s);
+    { cudaError_t me_ = cudaMemsetAsync(out, 0, 8, s); if (me_ != cudaSuccess) return me_; }
     k_dose_sum<<<592, 256, 0, s>>>(dose, n, out);
     return cudaGetLastError();
 }
@@ -107,14 +107,14 @@ cudaError_t launch_dose_projection(const uint32_t* dose, uint32_t vc, int axis, 
 
 cudaError_t launch_voxel_ssb(const DoseDna& d, const uint32_t* dose, uint32_t vc, double box_nm, float* lambda,
                              double* direct, cudaStream_t s) {
-    cudaMemsetAsync(direct, 0, 8, s);
+    { cudaError_t me_ = cudaMemsetAsync(direct, 0, 8, s); if (me_ != cudaSuccess) return me_; }
     k_voxel_ssb<<<592, 256, 0, s>>>(d, dose, vc, box_nm, lambda, direct);
     return cudaGetLastError();
 }
 
 cudaError_t launch_expected_dsb(const DoseDna& d, const float* lambda, const uint8_t* hits, double* out,
                                 cudaStream_t s) {
-    cudaMemsetAsync(out, 0, 8, s);
+    { cudaError_t me_ = cudaMemsetAsync(out, 0, 8, s); if (me_ != cudaSuccess) return me_; }
     k_expected_dsb<<<(d.n_fibers * 32 + 127) / 128, 128, 0, s>>>(d, lambda, hits, out);
     return cudaGetLastError();
 }

@@ -1131,7 +1131,7 @@ int irt_warps(int device) { return blocks_for((const void*)k_irt_loop, device) *
 cudaError_t launch_scan_u32(const uint32_t* cnt, uint32_t n, unsigned long long* off, cudaStream_t s);
 
 cudaError_t launch_irt(const IArgs& a, int device, cudaStream_t s, cudaEvent_t* ev) {
-    cudaMemsetAsync(a.counters, 0, 4 * sizeof(uint32_t), s);
+    { cudaError_t me_ = cudaMemsetAsync(a.counters, 0, 4 * sizeof(uint32_t), s); if (me_ != cudaSuccess) return me_; }
     k_irt_load<<<blocks_for((const void*)k_irt_load, device), IB, 0, s>>>(a);
     cudaError_t e = launch_scan_u32(a.ttiles, a.nseg, a.toff, s);
     if (e != cudaSuccess) return e;
@@ -1151,13 +1151,13 @@ cudaError_t launch_irt(const IArgs& a, int device, cudaStream_t s, cudaEvent_t* 
 
 cudaError_t launch_group_keys(const float4* rad, unsigned long long n, unsigned long long* key, uint32_t* maxpid,
                               cudaStream_t s) {
-    cudaMemsetAsync(maxpid, 0, 4, s);
+    { cudaError_t me_ = cudaMemsetAsync(maxpid, 0, 4, s); if (me_ != cudaSuccess) return me_; }
     if (n) k_group_keys<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(rad, n, key, maxpid);
     return cudaGetLastError();
 }
 
 cudaError_t launch_seg_max(const unsigned long long* off, uint32_t nseg, unsigned long long* out, cudaStream_t s) {
-    cudaMemsetAsync(out, 0, 8, s);
+    { cudaError_t me_ = cudaMemsetAsync(out, 0, 8, s); if (me_ != cudaSuccess) return me_; }
     k_seg_max<<<148, 256, 0, s>>>(off, nseg, out);
     return cudaGetLastError();
 }

@@ -1,11 +1,13 @@
 // noalloc.cu -- direct SSB scoring that allocates no device memory.
 //
 // Some callers cannot call cudaMalloc: a host that runs under another
-// framework's memory pool or a fixed device-memory budget, or code that must
-// not allocate while it is being captured into a CUDA graph.  For them this
+// framework's memory pool, or one held to a fixed device-memory budget.  For
+// them this
 // entry point runs the same scoring kernels as wgdna_score_direct on the
 // caller's device buffers, with its scratch in a fixed array that every GPU
-// loading this library holds until the process exits.
+// loading this library holds until the process exits.  The first call on a
+// device looks up the array's device address; make that call before any
+// stream capture.
 #include <cstring>
 #include <mutex>
 

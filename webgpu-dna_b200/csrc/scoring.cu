@@ -289,7 +289,10 @@ __global__ void k_cluster(const uint8_t* hits, uint32_t n_per, uint32_t n_bp, ui
 cudaError_t launch_score(const float4* rad, const uint32_t* alive, unsigned long long n, const DnaDev& d,
                          double r_d, double p, int dedupe, uint32_t s0, uint32_t* hits_words,
                          const ScoreScratch& sc, cudaStream_t s) {
-    cudaMemsetAsync(sc.u64, 0, 8 * sizeof(unsigned long long), s);
+    // the result counters must start at zero: a failed clear would leave the
+    // previous call's counts to be read back
+    cudaError_t e = cudaMemsetAsync(sc.u64, 0, 8 * sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return e;
     if (n == 0) return cudaGetLastError();
     unsigned long long ntiles = (n + STILE - 1) / STILE;
     k_prep<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(rad, alive, n, d, r_d, dedupe, sc.info);
@@ -301,8 +304,11 @@ cudaError_t launch_score(const float4* rad, const uint32_t* alive, unsigned long
 
 cudaError_t launch_cluster(const uint8_t* hits, const DnaDev& d, uint32_t n_fibers, uint32_t* out, cudaStream_t s) {
     size_t sm = (size_t)d.n_bp_per * 8;
-    static bool attr = false;
-    if (!attr) { cudaFuncSetAttribute(k_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); attr = true; }
+    static DeviceOnce attr;
+    cudaError_t e = attr.run([] {
+        return cudaFuncSetAttribute(k_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    });
+    if (e != cudaSuccess) return e;
     k_cluster<<<n_fibers, 256, sm, s>>>(hits, d.n_bp_per, d.n_bp, out);
     return cudaGetLastError();
 }

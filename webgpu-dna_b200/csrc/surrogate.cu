@@ -470,22 +470,22 @@ cudaError_t launch_descriptors(const DescArgs& a, cudaStream_t s) {
 
 cudaError_t launch_sg_forward(const SgFwdArgs& a, cudaStream_t s) {
     if (a.n == 0) return cudaSuccess;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_sg_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536 + 1024);
-        attr = true;
-    }
+    static DeviceOnce attr;
+    cudaError_t e = attr.run([] {
+        return cudaFuncSetAttribute(k_sg_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536 + 1024);
+    });
+    if (e != cudaSuccess) return e;
     k_sg_fwd<<<(a.n + SG_TILE - 1) / SG_TILE, SG_TILE, 65536 + 1024, s>>>(a);
     return cudaGetLastError();
 }
 
 cudaError_t launch_sg_backward(const SgBwdArgs& a, cudaStream_t s) {
     if (a.n == 0) return cudaSuccess;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_sg_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 131072 + 1024);
-        attr = true;
-    }
+    static DeviceOnce attr;
+    cudaError_t e = attr.run([] {
+        return cudaFuncSetAttribute(k_sg_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 131072 + 1024);
+    });
+    if (e != cudaSuccess) return e;
     k_sg_bwd<<<(a.n + SG_TILE - 1) / SG_TILE, SG_TILE, 131072 + 1024, s>>>(a);
     return cudaGetLastError();
 }
@@ -512,7 +512,7 @@ cudaError_t launch_sg_standardise(const float* in, float* out, uint64_t n, int d
 
 cudaError_t launch_sg_reduce(const float* Y, uint32_t n, const float* ymean, const float* ystd, const float* E,
                              float E0, double* acc, cudaStream_t s) {
-    cudaMemsetAsync(acc, 0, (SG_OUT + 1) * sizeof(double), s);
+    { cudaError_t me_ = cudaMemsetAsync(acc, 0, (SG_OUT + 1) * sizeof(double), s); if (me_ != cudaSuccess) return me_; }
     const uint32_t nb = (n + 255) / 256 < 296u ? (n + 255) / 256 : 296u;
     if (n) k_sg_reduce<<<nb, 256, 0, s>>>(Y, n, ymean, ystd, E, E0, acc);
     return cudaGetLastError();

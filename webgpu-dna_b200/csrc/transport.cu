@@ -965,16 +965,19 @@ size_t transport_smem_bytes() {
     return S_TOTAL_PAD * 4 + TW * STG * 16 + TW * STG * 8 + TW * STASH * sizeof(StashRec) + 2 * TW * 4 + 24 * 4;
 }
 
+// resident CTAs of k_transport on `device` (the current device); the shared
+// memory attribute is set on each device the first time
 int transport_blocks(int device) {
-    static int cached = -1;
-    if (cached > 0) return cached;
+    static DeviceOnce attr;
+    attr.run([] {
+        return cudaFuncSetAttribute(k_transport, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)transport_smem_bytes());
+    });
     int sms = 0, per = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    cudaFuncSetAttribute(k_transport, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)transport_smem_bytes());
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_transport, TB, transport_smem_bytes());
     if (per < 1) per = 1;
-    cached = sms * per;
-    return cached;
+    return sms * per;
 }
 
 cudaError_t launch_transport(const TArgs& a, int blocks, cudaStream_t s) {
@@ -985,17 +988,18 @@ cudaError_t launch_transport(const TArgs& a, int blocks, cudaStream_t s) {
 cudaError_t launch_canon(const unsigned long long* key, const float4* rad, unsigned long long n, uint32_t np,
                          uint32_t* cnt, unsigned long long* off, uint32_t* cur, uint32_t* perm, float4* out,
                          uint32_t* err, cudaStream_t s) {
-    cudaMemsetAsync(cnt, 0, (size_t)np * 4, s);
-    cudaMemsetAsync(cur, 0, (size_t)np * 4, s);
+    cudaError_t e = cudaMemsetAsync(cnt, 0, (size_t)np * 4, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(cur, 0, (size_t)np * 4, s);
+    if (e != cudaSuccess) return e;
     if (n) k_pid_hist<<<1184, 256, 0, s>>>(key, n, cnt);
     k_scan<<<1, 1024, 0, s>>>(cnt, np, off);
     if (n) {
         k_scatter<<<1184, 256, 0, s>>>(key, n, off, cur, perm);
-        static bool attr = false;
-        if (!attr) {
-            cudaFuncSetAttribute(k_segsort, cudaFuncAttributeMaxDynamicSharedMemorySize, SEG_MAX * 12);
-            attr = true;
-        }
+        static DeviceOnce attr;
+        e = attr.run([] {
+            return cudaFuncSetAttribute(k_segsort, cudaFuncAttributeMaxDynamicSharedMemorySize, SEG_MAX * 12);
+        });
+        if (e != cudaSuccess) return e;
         k_segsort<<<np, 1024, SEG_MAX * 12, s>>>(key, rad, perm, off, out, err);
     }
     return cudaGetLastError();
@@ -1008,7 +1012,7 @@ cudaError_t launch_scan_u32(const uint32_t* cnt, uint32_t n, unsigned long long*
 
 cudaError_t launch_reduce(const float* results, uint32_t np, const uint32_t* dose, uint32_t nvox,
                           unsigned long long* out, cudaStream_t s) {
-    cudaMemsetAsync(out, 0, 16, s);
+    { cudaError_t me_ = cudaMemsetAsync(out, 0, 16, s); if (me_ != cudaSuccess) return me_; }
     k_reduce<<<592, 256, 0, s>>>(results, np, dose, nvox, out);
     return cudaGetLastError();
 }

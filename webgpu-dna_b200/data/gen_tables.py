@@ -38,7 +38,11 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_SRC = os.environ.get("WGDNA_REFERENCE_WGSL", "/root/reference/public/cross_sections.wgsl")
+# the reference's table source: WGDNA_REFERENCE_WGSL, else public/cross_sections.wgsl
+# under the checkout named by WGDNA_REFERENCE, else the command-line argument
+DEFAULT_SRC = os.environ.get("WGDNA_REFERENCE_WGSL") or (
+    os.path.join(os.environ["WGDNA_REFERENCE"], "public", "cross_sections.wgsl")
+    if os.environ.get("WGDNA_REFERENCE") else None)
 MAGIC = b"WGDNAXS1"
 ENTRY_FMT = "<24sIIII"
 
@@ -107,6 +111,9 @@ def manifest(arrays):
 
 def main(argv):
     src = argv[1] if len(argv) > 1 else DEFAULT_SRC
+    if not src:
+        sys.exit("usage: gen_tables.py <reference>/public/cross_sections.wgsl "
+                 "(or set WGDNA_REFERENCE to the reference checkout)")
     with open(src) as f:
         arrays = parse_wgsl(f.read())
     blob = build_blob(arrays)
