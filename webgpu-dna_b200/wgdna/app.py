@@ -26,6 +26,18 @@ def ensure_pipelines(np_, log=_nolog):
     return _cache
 
 
+def damage_numbers(total_deposited_eV, box_nm, n_bp, ssb_dir, ssb_ind, dsb):
+    """The arithmetic of scoreDamageAt10keV (app.ts:190-194): box dose in Gy
+    over the full edge 2 * box_nm (box_nm is the half-width), DSB per Gy per
+    Gbp of target, DSB / SSB."""
+    dose_box_Gy = (total_deposited_eV * 1.602e-19) / (((2 * box_nm * 1e-9) ** 3) * 1000)
+    target_Gbp = n_bp * 1e-9
+    dsb_per_gy_gbp = dsb / (dose_box_Gy * target_Gbp) if dose_box_Gy > 0 else 0.0
+    ssb_tot = ssb_dir + ssb_ind
+    frac = dsb / ssb_tot if ssb_tot > 0 else 0.0
+    return dose_box_Gy, dsb_per_gy_gbp, frac
+
+
 def score_damage_at_10kev(ctx, dna, chem, rad_buf, rad_n, total_deposited_eV, box_nm, rng, log, kernel_dna_hits):
     """scoreDamageAt10keV (app.ts:167-207)."""
     if chem.get("chem_pos_final") is not None and chem.get("chem_alive_final") is not None:
@@ -38,11 +50,7 @@ def score_damage_at_10kev(ctx, dna, chem, rad_buf, rad_n, total_deposited_eV, bo
     ssb_dir = direct["ssb_count"]
     ssb_ind = indirect["ssb0"] + indirect["ssb1"]
     dsb = clust["dsb"]
-    dose_box_Gy = (total_deposited_eV * 1.602e-19) / (((2 * box_nm * 1e-9) ** 3) * 1000)
-    target_Gbp = dna.n_bp * 1e-9
-    dsb_per_gy_gbp = dsb / (dose_box_Gy * target_Gbp) if dose_box_Gy > 0 else 0.0
-    ssb_tot = ssb_dir + ssb_ind
-    frac = dsb / ssb_tot if ssb_tot > 0 else 0.0
+    dose_box_Gy, dsb_per_gy_gbp, frac = damage_numbers(total_deposited_eV, box_nm, dna.n_bp, ssb_dir, ssb_ind, dsb)
     log(f"    DAMAGE: SSB_dir={ssb_dir}  SSB_ind={ssb_ind}  DSB={dsb}  (DSB/SSB={frac:.3f})  "
         f"box_dose={dose_box_Gy:.3f} Gy  target={dna.n_bp / 1e6:.1f} Mbp  reach_dir={direct['in_reach']} "
         f"reach_ind={indirect['in_reach']}  kernel_hits={kernel_dna_hits or 0}", "data")

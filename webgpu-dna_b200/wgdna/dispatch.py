@@ -60,6 +60,31 @@ def aggregate(results, E_eV):
     }
 
 
+def energy_summary(E_eV, np_, results, dose_units, counters, sec_n, rad_n_raw, max_rad):
+    """The readback arithmetic of runAtEnergy (dispatch.ts:178-226): deposited
+    energy from the u32 dose grid (x100 per eV), initial G per 100 eV of it,
+    the per-primary means over non-escaped primaries and the conservation
+    ratio against n_therm * E.  ``dose_units`` is the grid's integer sum."""
+    total_deposited_eV = dose_units / 100.0
+    per100 = total_deposited_eV / 100.0
+    agg = aggregate(results, E_eV)
+    expected = agg["n_therm"] * E_eV
+    rad_n_stored = min(int(rad_n_raw), int(max_rad))
+    return {
+        **agg,
+        "total_deposited_eV": total_deposited_eV, "expected_deposited_eV": expected,
+        "cons_ratio": total_deposited_eV / expected if expected > 0 else 0.0,
+        "rad_OH": int(counters[0]), "rad_eaq": int(counters[1]), "rad_H": int(counters[2]),
+        "G_OH": counters[0] / per100 if per100 > 0 else 0.0,
+        "G_eaq": counters[1] / per100 if per100 > 0 else 0.0,
+        "G_H": counters[2] / per100 if per100 > 0 else 0.0,
+        "kernel_dna_hits": int(counters[4]),
+        "rad_n_raw": int(rad_n_raw), "rad_n_stored": rad_n_stored,
+        "rad_dropped": max(0, int(rad_n_raw) - int(max_rad)),
+        "sec_per_pri": sec_n / np_,
+    }
+
+
 def run_at_energy(ctx, E_eV, np_, box_nm, ce_eV, dna=None, run_chemistry=None, seed=None, keep_rad=True):
     """runAtEnergy: transport on the GPU, readbacks, optional chemistry callback
     (called only at 10 keV, dispatch.ts:244).  ``run_chemistry`` may be the
@@ -77,24 +102,15 @@ def run_at_energy(ctx, E_eV, np_, box_nm, ce_eV, dna=None, run_chemistry=None, s
                L.wgdna_transport_copy_out(ctx.h, _lib.ptr(results), _lib.ptr(dose),
                                           _lib.ptr(rad) if keep_rad else None,
                                           st.rad_n_stored if keep_rad else 0, C.byref(n)))
-    total_deposited_eV = st.dep_units / 100.0
-    per100 = total_deposited_eV / 100.0
-    agg = aggregate(results, E_eV)
-    expected = agg["n_therm"] * E_eV
+    summ = energy_summary(E_eV, np_, results, st.dep_units, list(st.counters), st.sec_n, st.rad_n_raw, ctx.max_rad)
+    agg = {k: summ[k] for k in ("n_therm", "n_esc", "mean_total", "mean_prod", "mean_sp", "mean_ions")}
     out = {
-        "E": E_eV, **agg,
+        "E": E_eV, **summ,
         "dt": 0.0, "t_prim": st.ms_transport, "t_sec": 0.0,
-        "sec_n": int(st.sec_n), "sec_dropped": int(st.sec_dropped), "sec_per_pri": st.sec_n / np_,
+        "sec_n": int(st.sec_n), "sec_dropped": int(st.sec_dropped),
         "sec_terminated_cutoff": int(st.sec_stats[1]), "sec_terminated_bounds": int(st.sec_stats[2]),
         "sec_steps": int(st.sec_stats[3]), "sec_tertiary_ions": int(st.sec_stats[4]),
-        "total_deposited_eV": total_deposited_eV, "expected_deposited_eV": expected,
-        "cons_ratio": total_deposited_eV / expected if expected > 0 else 0.0,
-        "rad_OH": int(st.counters[0]), "rad_eaq": int(st.counters[1]), "rad_H": int(st.counters[2]),
-        "G_OH": st.counters[0] / per100 if per100 > 0 else 0.0,
-        "G_eaq": st.counters[1] / per100 if per100 > 0 else 0.0,
-        "G_H": st.counters[2] / per100 if per100 > 0 else 0.0,
-        "rad_n_raw": int(st.rad_n_raw), "rad_n_stored": int(st.rad_n_stored), "rad_dropped": int(st.rad_dropped),
-        "kernel_dna_hits": int(st.counters[4]), "chem_result": None, "rad_buf_final": rad,
+        "chem_result": None, "rad_buf_final": rad,
         "dose_arr": dose if E_eV == 10000 else None, "results": results, "stats": st,
         "dep_eV_f64": st.dep_eV_f64, "steps": int(st.steps),
     }
