@@ -278,6 +278,8 @@ def run_native(args, ws, rank, local):
         e2e_s = float(t.item())
     e2e_value = ws * NPr * args.steps / e2e_s
 
+    physics = physics_fields(ctx, L, p, NPr) if rank == 0 else None
+
     # roofline of the dominant kernel: algorithmic bytes per launch / its mean duration
     pk = peaks()
     mean = lambda a: sum(a) / len(a)
@@ -327,6 +329,7 @@ def run_native(args, ws, rank, local):
                          "alg_bytes": int(alg),
                          "peak_source": "fallback" if pk.get("fallback") else "measured"},
             "clocks": clocks,
+            "physics": physics,
             "job": {"ssb": job.get("ssb"), "dsb": job.get("dsb"), "in_reach": job.get("reach")} if ws > 1 else None,
             "work": {"rad_n": int(R), "sec_n": int(S), "steps": int(st.steps), "irt_pairs": int(ir.n_pairs),
                      "irt_events": int(ir.n_events), "irt_init_events": int(Ei), "irt_species": int(Np),
@@ -342,6 +345,68 @@ def run_native(args, ws, rank, local):
                                               f"transport+IRT+scoring (oracle, {nthreads} threads)"}
         print(json.dumps(line), flush=True)
     ctx.close()
+
+
+PUBLISHED_10KEV = os.path.join(ROOT, "tests", "golden", "reference_outputs.json")
+
+
+def physics_fields(ctx, L, p, npr):
+    """The physics of one more (untimed) step of the same workload, against the
+    reference's published 10 keV run (validation/webgpu-results.json:6-30):
+    CSDA, ions per primary, initial G, G(1 us), SSB_dir, DSB, kernel hits, each
+    with z = (ours - published) / sigma, sigma = the per-track standard
+    deviation times sqrt(1/n + 1/4096) (Poisson for SSB_dir and DSB)."""
+    import ctypes as C
+    import numpy as np
+    from wgdna import _lib
+    pub = json.load(open(PUBLISHED_10KEV))["webgpu_10keV"]
+    st, ir, ssb, dsb = _lib.TransportStats(), _lib.IrtResult(), _lib.SsbResult(), _lib.DsbResult()
+    _lib.check("wgdna_transport", L.wgdna_transport(ctx.h, C.byref(p), C.byref(st)))
+    res = np.zeros(npr * 8, np.float32)
+    rad = np.zeros((st.rad_n_stored, 4), np.float32)
+    n = C.c_uint64()
+    _lib.check("copy_out", L.wgdna_transport_copy_out(ctx.h, _lib.ptr(res), None, _lib.ptr(rad), st.rad_n_stored,
+                                                       C.byref(n)))
+    L.wgdna_irt_record_curves(ctx.h, 1)
+    try:
+        _lib.check("wgdna_irt", L.wgdna_irt(ctx.h, st.n_therm, E_EV, 1 + p.seed, C.byref(ir)))
+        cv = np.zeros((npr, 16, 5), np.float32)
+        _lib.check("wgdna_irt_curves", L.wgdna_irt_curves(ctx.h, _lib.ptr(cv), npr, C.byref(n)))
+    finally:
+        L.wgdna_irt_record_curves(ctx.h, 0)
+    _lib.check("wgdna_score", L.wgdna_score(ctx.h, 0x12345678, C.byref(ssb), C.byref(dsb)))
+    r = res.reshape(-1, 8)
+    ru = r.view(np.uint32)
+    th = ru[:, 5] == 0
+    nth = int(th.sum())
+    f = math.sqrt(1.0 / max(nth, 1) + 1.0 / 4096)
+    out = {"n_therm": nth, "e_conservation": st.dep_units / 100.0 / (nth * E_EV) if nth else None}
+
+    def put(name, val, ref, sig):
+        out[name] = {"value": round(float(val), 4), "published": ref,
+                     "z": round(float((val - ref) / sig), 3) if sig > 0 else None}
+
+    path, ions = r[th, 0].astype(np.float64), ru[th, 3].astype(np.float64)
+    put("csda_nm", path.mean(), pub["tracking"]["csdaNm"], path.std() * f)
+    put("ions_per_primary", ions.mean(), pub["tracking"]["ionsPerPriPrimaryOnly"], ions.std() * f)
+    per100 = st.dep_units / 1e4
+    w = np.rint(rad[:, 3]).astype(np.int64)
+    pid, code = w >> 3, w & 7
+    for k, name, codes in ((0, "G_OH_init", [0]), (1, "G_eaq_init", [1, 5]), (2, "G_H_init", [2])):
+        cnt = np.bincount(pid[np.isin(code, codes)], minlength=npr).astype(np.float64)
+        put(name, st.counters[k] / per100, pub["pre_chemistry"][name], cnt.std() / 100.0 * f)
+    per_track = cv[:, 15, :].astype(np.float64) / (E_EV / 100.0)
+    for j, sp in enumerate(("G_OH", "G_eaq", "G_H", "G_H2O2", "G_H2")):
+        put(sp + "_1us", ir.G[6][j], pub["chemistry_1us"][sp], per_track[:, j].std() * f)
+    d = pub["dna_damage"]
+    for name, got, ref in (("SSB_dir", ssb.ssb, d["SSB_dir"]), ("DSB", dsb.dsb, d["DSB"])):
+        put(name, got, ref, math.sqrt(got + ref))
+    out["kernel_hits"] = {"value": int(st.counters[4]), "published": d["kernelHits"]}
+    zs = [abs(v["z"]) for v in out.values() if isinstance(v, dict) and v.get("z") is not None]
+    out["max_abs_z"] = max(zs) if zs else None
+    out["source"] = ("published: validation/webgpu-results.json:6-30 (4096 x 10 keV, cutoff 7.4 eV, the "
+                     "reference's own generator); ours: one untimed step of this workload")
+    return out
 
 
 def _irt_alg_bytes(ir):

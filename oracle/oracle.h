@@ -55,7 +55,7 @@ typedef struct {
     uint64_t rad_n;
     uint64_t dep_units;     /* sum of all in-grid u32(dep*100) deposits */
     double dep_eV_f64;      /* sum of every deposit (f64), in or out of the grid */
-    uint64_t sec_n;         /* secondaries emitted (counters[6]) */
+    uint64_t sec_n;         /* secondaries kept: min(counters[6] emitted, max_sec) */
     uint64_t steps;         /* electron steps taken (primary + secondary) */
 } orc_transport_out;
 

@@ -228,6 +228,7 @@ typedef struct {
     sink_t *sk;
     uint32_t pid, sub, seq;
     float pidf;             /* f32(pid)*8.0 */
+    uint32_t *sec_next;     /* the run's sec_buf index (counters[6] of primary.wgsl), shared */
 } emit_t;
 
 static void put(emit_t *e, float x, float y, float z, float code) {
@@ -441,42 +442,49 @@ static int interact(emit_t *e, rng_t *s, float *pE, float px, float py, float pz
                     }
                 }
                 if (W_sec > p->ce_eV) {
-                    uint32_t sec_idx = c[6]++;
-                    (void)sec_idx;        /* the cap is applied after the run (oracle.h) */
-                    float E_before = E + bind + W_sec;
-                    float cos_s;
-                    if (W_sec < 50.0f) {
-                        cos_s = 2.0f * rf(s) - 1.0f;
-                    } else if (W_sec <= 200.0f) {
-                        if (rf(s) <= 0.1f) cos_s = 2.0f * rf(s) - 1.0f;
-                        else cos_s = rf(s) * 0.70710678f;
-                    } else {
-                        float sin2 = fminf(fmaxf((1.0f - W_sec / E_before) / (1.0f + W_sec / 1022000.0f), 0.0f), 1.0f);
-                        cos_s = sqrtf(fmaxf(0.0f, 1.0f - sin2));
-                    }
-                    float sin_s = sqrtf(fmaxf(0.0f, 1.0f - cos_s * cos_s));
-                    float sps, cps; om_sincosf(TWO_PI_F * rf(s), &sps, &cps);
-                    float sdx = *dx, sdy = *dy, sdz = *dz;
-                    rotate(&sdx, &sdy, &sdz, cos_s, sin_s, cps, sps);
-                    float p_inc = sqrtf(E_before), p_sec = sqrtf(W_sec);
-                    float pfx = p_inc * *dx - p_sec * sdx;
-                    float pfy = p_inc * *dy - p_sec * sdy;
-                    float pfz = p_inc * *dz - p_sec * sdz;
-                    float pfl = sqrtf(pfx * pfx + pfy * pfy + pfz * pfz);
-                    if (pfl > 1e-10f) { *dx = pfx / pfl; *dy = pfy / pfl; *dz = pfz / pfl; }
-                    if (secs->n == secs->cap) {
-                        secs->cap = secs->cap ? secs->cap * 2 : 256;
-                        secs->v = (sec_t *)realloc(secs->v, secs->cap * sizeof(sec_t));
-                    }
-                    sec_t *q = &secs->v[secs->n++];
-                    q->x = px; q->y = py; q->z = pz; q->E = W_sec;
-                    q->dx = sdx; q->dy = sdy; q->dz = sdz;
-                    if (s->mode == 1) {           /* child state = 4 parent draws */
-                        memset(&q->r, 0, sizeof q->r);
-                        q->r.mode = 1;
-                        for (int j = 0; j < 4; ++j) q->r.s[j] = rn(s);
-                    } else {
-                        rng_philox(&q->r, p->seed, e->pid, secs->n);
+                    /* primary.wgsl:363-364: every emission takes a sec_buf index;
+                     * at or beyond max_sec the secondary is dropped together with
+                     * its angle draws and the primary's momentum update.  Which
+                     * emissions come last depends on the order the primaries run
+                     * in, as in the reference. */
+                    c[6]++;
+                    uint32_t sec_idx = __atomic_fetch_add(e->sec_next, 1u, __ATOMIC_RELAXED);
+                    if (sec_idx < p->max_sec) {
+                        float E_before = E + bind + W_sec;
+                        float cos_s;
+                        if (W_sec < 50.0f) {
+                            cos_s = 2.0f * rf(s) - 1.0f;
+                        } else if (W_sec <= 200.0f) {
+                            if (rf(s) <= 0.1f) cos_s = 2.0f * rf(s) - 1.0f;
+                            else cos_s = rf(s) * 0.70710678f;
+                        } else {
+                            float sin2 = fminf(fmaxf((1.0f - W_sec / E_before) / (1.0f + W_sec / 1022000.0f), 0.0f), 1.0f);
+                            cos_s = sqrtf(fmaxf(0.0f, 1.0f - sin2));
+                        }
+                        float sin_s = sqrtf(fmaxf(0.0f, 1.0f - cos_s * cos_s));
+                        float sps, cps; om_sincosf(TWO_PI_F * rf(s), &sps, &cps);
+                        float sdx = *dx, sdy = *dy, sdz = *dz;
+                        rotate(&sdx, &sdy, &sdz, cos_s, sin_s, cps, sps);
+                        float p_inc = sqrtf(E_before), p_sec = sqrtf(W_sec);
+                        float pfx = p_inc * *dx - p_sec * sdx;
+                        float pfy = p_inc * *dy - p_sec * sdy;
+                        float pfz = p_inc * *dz - p_sec * sdz;
+                        float pfl = sqrtf(pfx * pfx + pfy * pfy + pfz * pfz);
+                        if (pfl > 1e-10f) { *dx = pfx / pfl; *dy = pfy / pfl; *dz = pfz / pfl; }
+                        if (secs->n == secs->cap) {
+                            secs->cap = secs->cap ? secs->cap * 2 : 256;
+                            secs->v = (sec_t *)realloc(secs->v, secs->cap * sizeof(sec_t));
+                        }
+                        sec_t *q = &secs->v[secs->n++];
+                        q->x = px; q->y = py; q->z = pz; q->E = W_sec;
+                        q->dx = sdx; q->dy = sdy; q->dz = sdz;
+                        if (s->mode == 1) {           /* child state = 4 parent draws */
+                            memset(&q->r, 0, sizeof q->r);
+                            q->r.mode = 1;
+                            for (int j = 0; j < 4; ++j) q->r.s[j] = rn(s);
+                        } else {
+                            rng_philox(&q->r, p->seed, e->pid, secs->n);
+                        }
                     }
                 }
             } else {
@@ -610,9 +618,9 @@ static void run_secondary(emit_t *e, sec_t *q) {                  /* secondary.w
     }
 }
 
-static void run_primary(const orc_transport_params *p, uint32_t idx, sink_t *sk, float *res) {
+static void run_primary(const orc_transport_params *p, uint32_t idx, sink_t *sk, float *res, uint32_t *sec_next) {
     uint32_t gid = p->pid_base + idx;
-    emit_t e = {p, sk, gid, 0, 0, (float)gid * 8.0f};
+    emit_t e = {p, sk, gid, 0, 0, (float)gid * 8.0f, sec_next};
     rng_t s;
     if (p->rng_mode == 1) rng_reference(&s, gid, (uint32_t)p->seed);
     else rng_philox(&s, p->seed, gid, 0);
@@ -676,6 +684,7 @@ int orc_transport(const orc_transport_params *p, orc_transport_out *o, int nthre
     uint32_t **tdose = (uint32_t **)calloc((size_t)nthreads, sizeof(uint32_t *));
     if (!sinks || !tdose) return -2;
     if (o->dose) memset(o->dose, 0, ngrid * 4);
+    uint32_t sec_next = 0;
 #pragma omp parallel num_threads(nthreads)
     {
         int tid = 0;
@@ -687,7 +696,7 @@ int orc_transport(const orc_transport_params *p, orc_transport_out *o, int nthre
 #pragma omp for schedule(dynamic, 1)
         for (int64_t i = 0; i < (int64_t)np; ++i) {
             sinks[i].dose = dl;
-            run_primary(p, (uint32_t)i, &sinks[i], o->results + 8 * i);
+            run_primary(p, (uint32_t)i, &sinks[i], o->results + 8 * i, &sec_next);
         }
     }
     memset(o->counters, 0, sizeof o->counters);
@@ -717,7 +726,7 @@ int orc_transport(const orc_transport_params *p, orc_transport_out *o, int nthre
         o->steps += s->steps;
         free(s->rad); free(s->key);
     }
-    o->sec_n = o->counters[6];
+    o->sec_n = o->counters[6] < p->max_sec ? o->counters[6] : p->max_sec;
     if (o->dose) {
         for (int t = 0; t < nthreads; ++t) {
             if (!tdose[t]) continue;

@@ -127,3 +127,17 @@ def test_damage_numbers_match_app_ts():
 def test_classify_matches_table_ts():
     for r in [0.0, 0.49, 0.5, 0.8999, 0.9, 1.0, 1.1, 1.1001, 2.0, 2.0001, float("inf")]:
         assert app.classify(r) == js_classify(r)
+
+
+def test_oracle_secondary_cap_counting():
+    """dispatch.ts:124-126 with the emission rule of primary.wgsl:363-364:
+    sec_n = min(emitted, MAX_SEC), sec_dropped = emitted - sec_n, and dropped
+    secondaries leave their energy undeposited."""
+    full = oracle.transport(16, 10000.0, seed=3, nthreads=1, want_dose=False)
+    cap = oracle.transport(16, 10000.0, seed=3, nthreads=1, want_dose=False, max_sec=300)
+    assert not full["capped"] and full["sec_n"] == full["counters"][6]
+    assert cap["capped"] and cap["sec_n"] == 300 and cap["counters"][6] > 300
+    assert cap["dep_eV_f64"] < full["dep_eV_f64"]
+    # primaries run one after another here: the first primaries keep every secondary
+    r0, r1 = full["results"].reshape(-1, 8), cap["results"].reshape(-1, 8)
+    assert np.array_equal(r0[0].view(np.uint32), r1[0].view(np.uint32))

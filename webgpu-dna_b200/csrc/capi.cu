@@ -336,9 +336,12 @@ extern "C" int wgdna_transport(wgdna_ctx* c, const wgdna_transport_params* p, wg
         st->rad_n_raw = hs.rad_next.v;
         st->rad_n_stored = stored;
         st->rad_dropped = hs.rad_next.v - stored;
+        // dispatch.ts:125-126: emitted, kept (at most max_sec), dropped; the
+        // global queue holds at most the kept ones, so sec_drop stays 0
+        const uint32_t kept = hs.sec_tail.v < c->cfg.max_sec ? hs.sec_tail.v : c->cfg.max_sec;
         st->sec_n_raw = hs.sec_tail.v;
-        st->sec_n = hs.sec_tail.v - hs.sec_drop;
-        st->sec_dropped = hs.sec_drop;
+        st->sec_n = kept - (hs.sec_drop < kept ? hs.sec_drop : kept);
+        st->sec_dropped = hs.sec_tail.v - st->sec_n;
         st->dep_units = red[0];
         st->dep_eV_f64 = hs.dep_f64;
         st->steps = hs.steps;

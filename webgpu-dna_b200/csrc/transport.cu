@@ -56,7 +56,7 @@ constexpr float PI_F = 3.14159265f;
 // counters inside the block's shared block: [0..7] counters, [8..15] sec_stats, [16..23] dbg
 enum { C_OH = 0, C_EAQ = 1, C_H = 2, C_H3O = 3, C_DNA = 4, C_H2 = 5,
        SS_CUT = 9, SS_BOUNDS = 10, SS_STEPS = 11, SS_TERT = 12,
-       D_IONS = 16, D_EXC = 17, D_ESC = 18, D_PRIM = 19, D_WSUM = 20, D_DOSE = 21, C_SECN = 22 };
+       D_IONS = 16, D_EXC = 17, D_ESC = 18, D_PRIM = 19, D_WSUM = 20, D_DOSE = 21 };
 
 struct Particle {
     float px, py, pz, E, dx, dy, dz;
@@ -399,9 +399,12 @@ __device__ __forceinline__ void interact(const TArgs& A, Blk& b, Particle& q, De
                     }
                 }
                 if (W_sec > A.ce) {                              // primary.wgsl:362-413
-                    atomicAdd(&b.cnt[C_SECN], 1u);
-                    q.nsec++;
-                    {
+                    // every emission takes a sec_buf index (counters[6]); at or
+                    // beyond max_sec the secondary is dropped together with its
+                    // angle draws and the primary's momentum update (:364)
+                    const uint32_t sec_idx = atomicAdd(&A.st->sec_tail.v, 1u);
+                    if (sec_idx < A.max_sec) {
+                        q.nsec++;
                         float E_before = E + bind + W_sec;
                         float cos_s;
                         if (W_sec < 50.0f) {
@@ -863,8 +866,7 @@ __global__ void __launch_bounds__(TB, 2) k_transport(TArgs A) {
     __syncthreads();
     if (threadIdx.x < 24 && cnt[threadIdx.x]) {
         uint32_t v = cnt[threadIdx.x];
-        if (threadIdx.x == C_SECN) atomicAdd(&S->sec_tail.v, v);
-        else if (threadIdx.x < 8) atomicAdd(&S->counters[threadIdx.x], v);
+        if (threadIdx.x < 8) atomicAdd(&S->counters[threadIdx.x], v);
         else if (threadIdx.x < 16) atomicAdd(&S->sec_stats[threadIdx.x - 8], v);
         else atomicAdd(&S->dbg[threadIdx.x - 16], v);
     }
