@@ -51,6 +51,45 @@ int wgdna_version(void);
 /* Run the context's work on a caller's cudaStream_t (NULL = the context's own). */
 int wgdna_set_stream(wgdna_ctx *ctx, void *cuda_stream);
 
+/* Launch and scheduling shapes of the kernels.  No counterpart in the
+ * reference (WebGPU picks none of these).  They change how work is spread over
+ * the GPU, never the results: every particle, pair and track draws from its
+ * own random stream.  wgdna_create reads them from data/tuning.txt next to the
+ * library when that file exists (written by `python -m wgdna.autotune`, one
+ * "key value" line per field below), else uses the defaults shown. */
+typedef struct {
+    uint32_t transport_ctas_per_sm;  /* resident transport CTAs per SM, 0 = as many as fit (2) */
+    uint32_t prim_take;              /* primaries a transport warp may start per iteration (2), 1..32 */
+    uint32_t stash_keep;             /* secondaries a warp keeps when its stash spills (16) */
+    uint32_t stash_spill;            /* stash level that spills to the global queue (32), <= 48;
+                                      * 0 = no stash: every secondary goes to the global queue */
+    uint32_t queue_poll;             /* a busy warp polls the global queue every queue_poll iterations (8),
+                                      * a power of two <= 1024 */
+    uint32_t irt_init_blocks_per_sm; /* resident blocks of the IRT pairing kernel per SM, 0 = as many as fit */
+    uint32_t irt_loop_blocks_per_sm; /* resident blocks of the IRT event kernel per SM, 0 = as many as fit */
+} wgdna_tuning;
+void wgdna_default_tuning(wgdna_tuning *t);
+int wgdna_get_tuning(wgdna_ctx *ctx, wgdna_tuning *t);
+int wgdna_set_tuning(wgdna_ctx *ctx, const wgdna_tuning *t);
+
+/* Bounds of the device-side waits.  No counterpart in the reference (its
+ * WebGPU queue has no device-side waits); for hosts that want a shorter
+ * watchdog and for failure-detection tests.  queue_ns: a transport lane's wait
+ * for a queued secondary to be published (default 2 s); idle_ns: a transport
+ * warp's wait without work before the run ends (default 30 s); mma_ns: a
+ * surrogate kernel's wait for its tensor-core step (default 1 s).  0 keeps the
+ * default.  A wait that runs out sets a bit of the stage's device_error and the
+ * call returns WGDNA_ERR_DEVICE; the context stays usable.  test_flags is 0 in
+ * normal use; WGDNA_TEST_UNPUBLISHED makes the transport publish its queued
+ * secondaries under an epoch that no consumer waits for (the queue wait runs
+ * out), WGDNA_TEST_MMA_WAIT makes each surrogate tile give up its first
+ * tensor-core wait before polling (the tile then waits, at most 1 s, for the
+ * tensor cores to finish before it reads or frees tensor memory). */
+#define WGDNA_TEST_UNPUBLISHED 1u
+#define WGDNA_TEST_MMA_WAIT 2u
+int wgdna_set_wait_limits(wgdna_ctx *ctx, uint64_t queue_ns, uint64_t idle_ns, uint64_t mma_ns,
+                          uint32_t test_flags);
+
 /* ---------------------------------------------------------------- Phase A+B */
 /* The uniform structs P (src/gpu/dispatch.ts:13-42) and SP (dispatch.ts:45-70). */
 typedef struct {

@@ -105,28 +105,43 @@ def test_irt_curves_bit_exact(ctx):
 
 @pytest.mark.gpu
 def test_trained_surrogate_against_irt(ctx):
-    """Train on the IRT's own curves at 3 and 10 keV, then check a held-out
-    batch: the surrogate's G(1 us) against the IRT's, and its time against the
-    IRT's on the same tracks (what the network gains over the method alone)."""
+    """Trained by the library's kernels with the recipe the benchmark uses
+    (~1e5 IRT tracks at 1, 3 and 10 keV), then one held-out 4096-track batch at
+    each energy: the batch G(t) within 2 % of the IRT's at every curve time and
+    species (where G > 0.05), and the surrogate chemistry at least 20 times
+    faster than the batched IRT on the same tracks (what the network gains over
+    the method alone)."""
     from wgdna import surrogate as S
-    Xs, Gs = [], []
-    seed = 500
-    for E in (3000.0, 10000.0):
-        for _ in range(3):
-            X, G, _, _ = S.track_data(ctx, np.full(4096, E, np.float32), seed)
-            seed += 11
-            Xs.append(X); Gs.append(G)
-    losses = S.fit(ctx, np.concatenate(Xs), np.concatenate(Gs), schedule=((25, 2e-3), (10, 5e-4)), seed=3)
-    assert losses[-1] < 0.8 * losses[0]
+    info = S.train_on_irt(ctx, 8)
+    assert info["loss_last"] < 0.5 * info["loss_first"]
+    for E in S.TRAIN_ENERGIES:
+        gi, gc, irt_ms, sg_ms, Xh = S.held_out(ctx, E, 424242 + int(E))
+        e1, eall = S.g_errors(gi, gc)
+        assert eall <= 0.02, (E, e1, eall)
+        assert irt_ms >= 20.0 * sg_ms, (E, irt_ms, sg_ms)
+        if E == 10000.0 and Xh.shape[0] == 4096:               # every track holds species
+            # the whole-batch device path matches the host-side prediction
+            gp = S.batch_G(S.predict(ctx, Xh), np.full(4096, E))
+            np.testing.assert_allclose(gc, gp, rtol=2e-3, atol=1e-4)
+
+
+@pytest.mark.gpu
+def test_out_of_range_batch_falls_back_to_the_irt(ctx):
+    """A network fitted at 10 keV only: a 10 keV batch stays in its range and
+    runs the surrogate; a 300 eV batch leaves it and runs the IRT, whose G at the
+    curve times that are also checkpoints (1 ps, 100 ps, 10 ns, 1 us) equals
+    a direct wgdna_irt call's."""
+    from wgdna import surrogate as S
+    X, G, _, _ = S.track_data(ctx, np.full(4096, 10000.0, np.float32), 9001)
+    S.fit(ctx, X, G, schedule=((3, 2e-3),), seed=2)
     L = _lib.lib()
-    Xh, Gh, Eh, ir = S.track_data(ctx, np.full(4096, 10000.0, np.float32), 424242)
-    gi, gp = S.batch_G(Gh, Eh), S.batch_G(S.predict(ctx, Xh), Eh)
-    rel = np.abs(gp[15] - gi[15]) / gi[15]
-    assert rel.max() < 0.05, (gi[15], gp[15])
-    # the whole-batch path on the device matches the host-side prediction
-    Gc = np.zeros(80)
-    ms = C.c_float()
-    _lib.check("chem", L.wgdna_surrogate_chemistry(ctx.h, _lib.ptr(Gc), C.byref(ms)))
-    if Xh.shape[0] == 4096:                                      # every track holds species
-        np.testing.assert_allclose(Gc.reshape(16, 5), gp, rtol=2e-3, atol=1e-4)
-    assert ms.value < ir.ms / 5, (ms.value, ir.ms)
+    for E, expect_sg in ((10000.0, True), (300.0, False)):
+        p = wgdna.transport_params(1024, E, 15000.0, 7.5, seed=77, dna_enable=0)
+        st = _lib.TransportStats()
+        _lib.check("wgdna_transport", L.wgdna_transport(ctx.h, C.byref(p), C.byref(st)))
+        Gc, used = S.chemistry(ctx, st.n_therm, E, seed=1)
+        assert used == expect_sg, E
+        if not used:
+            ir = _lib.IrtResult()
+            _lib.check("wgdna_irt", L.wgdna_irt(ctx.h, st.n_therm, E, 1, C.byref(ir)))
+            np.testing.assert_allclose(Gc[[0, 5, 10, 15]], np.array(ir.G)[[0, 2, 4, 6]], rtol=1e-12, atol=0)

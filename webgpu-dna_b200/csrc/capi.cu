@@ -56,6 +56,10 @@ struct wgdna_ctx {
     uint32_t* d_err = nullptr;            // canonicalisation / IRT / scoring error word
     uint32_t epoch = 0;
     int tblocks = 0;
+    // bounds of the device-side waits (wgdna_set_wait_limits) and test switches
+    unsigned long long wait_queue_ns = WG_QUEUE_WAIT_NS, wait_idle_ns = WG_IDLE_WAIT_NS, wait_mma_ns = WG_MMA_WAIT_NS;
+    uint32_t test_flags = 0;
+    wgdna_tuning tune{};                  // launch and scheduling shapes (wgdna_set_tuning)
     // last transport
     bool have_transport = false;
     uint32_t last_np = 0, last_nseg = 0, last_pid_base = 0, irt_pid_base = 0;
@@ -119,6 +123,70 @@ static std::string lib_dir() {
         if (k != std::string::npos) return p.substr(0, k);
     }
     return ".";
+}
+
+extern "C" void wgdna_default_tuning(wgdna_tuning* t) {
+    if (!t) return;
+    t->transport_ctas_per_sm = 0;
+    t->prim_take = 2;
+    t->stash_keep = 16;
+    t->stash_spill = 32;
+    t->queue_poll = 8;
+    t->irt_init_blocks_per_sm = 0;
+    t->irt_loop_blocks_per_sm = 0;
+}
+
+static bool tuning_ok(const wgdna_tuning& t) {
+    const bool pow2 = t.queue_poll && (t.queue_poll & (t.queue_poll - 1)) == 0;
+    const bool stash = t.stash_spill == 0 ? t.stash_keep == 0
+                                          : (t.stash_spill <= TRANSPORT_STASH && t.stash_keep < t.stash_spill);
+    return t.prim_take >= 1 && t.prim_take <= 32 && stash && pow2 && t.queue_poll <= 1024 &&
+           t.transport_ctas_per_sm <= 8 && t.irt_init_blocks_per_sm <= 32 && t.irt_loop_blocks_per_sm <= 32;
+}
+
+// data/tuning.txt: "key value" lines (wgdna_tuning's field names), '#' comments;
+// a missing file keeps the defaults, a malformed one is an error
+static int tuning_load(const std::string& path, wgdna_tuning* t) {
+    FILE* f = fopen(path.c_str(), "r");
+    if (!f) return WGDNA_OK;
+    char line[256];
+    int rc = WGDNA_OK;
+    while (rc == WGDNA_OK && fgets(line, sizeof line, f)) {
+        char key[64];
+        unsigned long v = 0;
+        if (line[0] == '#' || sscanf(line, "%63s", key) != 1) continue;
+        if (sscanf(line, "%63s %lu", key, &v) != 2) { rc = WGDNA_ERR_ARG; break; }
+        uint32_t* dst = !strcmp(key, "transport_ctas_per_sm") ? &t->transport_ctas_per_sm
+                      : !strcmp(key, "prim_take") ? &t->prim_take
+                      : !strcmp(key, "stash_keep") ? &t->stash_keep
+                      : !strcmp(key, "stash_spill") ? &t->stash_spill
+                      : !strcmp(key, "queue_poll") ? &t->queue_poll
+                      : !strcmp(key, "irt_init_blocks_per_sm") ? &t->irt_init_blocks_per_sm
+                      : !strcmp(key, "irt_loop_blocks_per_sm") ? &t->irt_loop_blocks_per_sm : nullptr;
+        if (!dst) { rc = WGDNA_ERR_ARG; break; }
+        *dst = (uint32_t)v;
+    }
+    fclose(f);
+    if (rc != WGDNA_OK || !tuning_ok(*t)) {
+        wg_set_error("wgdna_create: malformed tuning table %s", path.c_str());
+        return WGDNA_ERR_ARG;
+    }
+    return WGDNA_OK;
+}
+
+extern "C" int wgdna_get_tuning(wgdna_ctx* c, wgdna_tuning* t) {
+    if (!c || !t) { wg_set_error("wgdna_get_tuning: NULL argument"); return WGDNA_ERR_ARG; }
+    *t = c->tune;
+    return WGDNA_OK;
+}
+
+extern "C" int wgdna_set_tuning(wgdna_ctx* c, const wgdna_tuning* t) {
+    if (!c || !t) { wg_set_error("wgdna_set_tuning: NULL argument"); return WGDNA_ERR_ARG; }
+    if (!tuning_ok(*t)) { wg_set_error("wgdna_set_tuning: a field is out of range"); return WGDNA_ERR_ARG; }
+    WG_CUDA_OK(cudaSetDevice(c->device));
+    c->tune = *t;
+    c->tblocks = transport_blocks(c->device, t->transport_ctas_per_sm);
+    return WGDNA_OK;
 }
 
 extern "C" void wgdna_default_cfg(wgdna_cfg* c) {
@@ -201,7 +269,10 @@ extern "C" int wgdna_create(const wgdna_cfg* cfg, wgdna_ctx** out) {
     if (r == WGDNA_OK && cudaMemset(c->d_secq, 0, sizeof(SecRec) * (size_t)c0.max_sec) != cudaSuccess) r = WGDNA_ERR_CUDA;
     if (r == WGDNA_OK) r = wgdna_set_dna_target(c, 3000.0, 21, 150.0);
     if (r != WGDNA_OK) { wgdna_destroy(c); return r; }
-    c->tblocks = transport_blocks(c->device);
+    wgdna_default_tuning(&c->tune);
+    r = tuning_load(lib_dir() + "/data/tuning.txt", &c->tune);
+    if (r != WGDNA_OK) { wgdna_destroy(c); return r; }
+    c->tblocks = transport_blocks(c->device, c->tune.transport_ctas_per_sm);
     *out = c;
     return WGDNA_OK;
 }
@@ -216,6 +287,22 @@ int ctx_view(wgdna_ctx* c, wg::CtxView* v) {
     v->Eprim = c->last_has_eprim ? c->d_Eprim : nullptr;
     v->E0 = c->last_E;
     v->sg = &c->sg;
+    v->mma_ns = c->wait_mma_ns;
+    v->mma_give_up_first = (c->test_flags & WGDNA_TEST_MMA_WAIT) != 0;
+    return WGDNA_OK;
+}
+
+extern "C" int wgdna_set_wait_limits(wgdna_ctx* c, uint64_t queue_ns, uint64_t idle_ns, uint64_t mma_ns,
+                                     uint32_t test_flags) {
+    if (!c) { wg_set_error("wgdna_set_wait_limits: NULL context"); return WGDNA_ERR_ARG; }
+    if (test_flags & ~(uint32_t)(WGDNA_TEST_UNPUBLISHED | WGDNA_TEST_MMA_WAIT)) {
+        wg_set_error("wgdna_set_wait_limits: unknown test flags 0x%x", test_flags);
+        return WGDNA_ERR_ARG;
+    }
+    c->wait_queue_ns = queue_ns ? queue_ns : WG_QUEUE_WAIT_NS;
+    c->wait_idle_ns = idle_ns ? idle_ns : WG_IDLE_WAIT_NS;
+    c->wait_mma_ns = mma_ns ? mma_ns : WG_MMA_WAIT_NS;
+    c->test_flags = test_flags;
     return WGDNA_OK;
 }
 
@@ -248,6 +335,13 @@ static TArgs make_targs(wgdna_ctx* c, const wgdna_transport_params* p) {
     a.dna_rise = p->dna_rise; a.dna_spacing = p->dna_spacing; a.dna_x0 = p->dna_x0; a.dna_r_bb = p->dna_r_bb;
     a.sec_steps = p->sec_steps; a.k0 = (uint32_t)p->seed; a.k1 = (uint32_t)(p->seed >> 32); a.epoch = c->epoch;
     a.pid_base = p->pid_base;
+    a.pub_epoch = (c->test_flags & WGDNA_TEST_UNPUBLISHED) ? c->epoch + 0x80000000u : c->epoch;
+    a.ready_ns = c->wait_queue_ns;
+    a.idle_ns = c->wait_idle_ns;
+    a.prim_take = c->tune.prim_take;
+    a.stash_keep = c->tune.stash_keep;
+    a.stash_spill = c->tune.stash_spill;
+    a.poll_mask = c->tune.queue_poll - 1;
     a.tab = c->tab;
     a.E_prim = p->E_per_primary ? c->d_Eprim : nullptr;
     a.results = c->d_results; a.dose = c->d_dose; a.rad = c->d_rad_raw; a.key = c->d_key;
@@ -396,7 +490,8 @@ static int irt_ensure(wgdna_ctx* c, uint32_t nseg, uint64_t rad_n, uint32_t cap)
     size_t slots = 2 * (size_t)rad_n + 64 * (size_t)nseg;
     size_t evslots = 16 * (size_t)rad_n + 2048 * (size_t)nseg;
     uint32_t hcap = cap * 8u + 4096u;
-    size_t hov = (size_t)irt_warps(c->device) * hcap;
+    const IrtShape shape{c->tune.irt_init_blocks_per_sm, c->tune.irt_loop_blocks_per_sm};
+    size_t hov = (size_t)irt_warps(c->device, shape) * hcap;
     if (slots > c->irt_slots) {
         TRY(dalloc(&c->d_px, slots)); TRY(dalloc(&c->d_py, slots)); TRY(dalloc(&c->d_pz, slots));
         TRY(dalloc(&c->d_tb, slots)); TRY(dalloc(&c->d_sp, slots)); TRY(dalloc(&c->d_alive8, slots));
@@ -411,7 +506,7 @@ static int irt_ensure(wgdna_ctx* c, uint32_t nseg, uint64_t rad_n, uint32_t cap)
         TRY(dalloc(&c->d_hov_t, hov)); TRY(dalloc(&c->d_hov_ab, hov));
         c->irt_hov = hov;
     }
-    c->irt_hcap = (uint32_t)(hov / irt_warps(c->device));
+    c->irt_hcap = (uint32_t)(hov / irt_warps(c->device, shape));
     if (slots > c->irt_pf_slots) {
         TRY(dalloc(&c->d_pf, slots));
         TRY(dalloc(&c->d_rec, 6 * slots));
@@ -466,7 +561,8 @@ static int irt_run(wgdna_ctx* c, uint32_t nseg, uint32_t n_therm, double E_eV, u
         c->curves_n = nseg;
     }
     WG_CUDA_OK(cudaEventRecord(c->ev[4], s));
-    WG_CUDA_OK(launch_irt(a, c->device, s, &c->ev[8]));
+    WG_CUDA_OK(launch_irt(a, c->device, IrtShape{c->tune.irt_init_blocks_per_sm, c->tune.irt_loop_blocks_per_sm},
+                          s, &c->ev[8]));
     WG_CUDA_OK(cudaEventRecord(c->ev[5], s));
     double tl[35];
     unsigned long long acc[16];

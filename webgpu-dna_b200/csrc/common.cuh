@@ -19,6 +19,13 @@ enum : uint32_t {
     DERR_SEG_SORT = 1u << 5,       // a rad_buf segment exceeded the sort capacity
 };
 
+// Default bounds of the device-side waits (wgdna_set_wait_limits changes them
+// per context): a lane waiting for a queued secondary, a transport warp without
+// work, a surrogate kernel waiting for its tensor-core step.
+constexpr unsigned long long WG_QUEUE_WAIT_NS = 2000000000ull;   // 2 s
+constexpr unsigned long long WG_IDLE_WAIT_NS = 30000000000ull;   // 30 s
+constexpr unsigned long long WG_MMA_WAIT_NS = 1000000000ull;     // 1 s
+
 // Cross-section tables (public/cross_sections.wgsl:9-72) in device memory.
 struct Tables {
     // small tables, copied to shared memory by the transport kernel, in this order

@@ -945,6 +945,7 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
                 int qn = 0;
                 const ProdCtx P{px, py, pz, tb, Di, id, pid, A.k0, A.k1};
                 const float etf = (float)et, dtm = 1e-4f + 1e-6f * etf;
+                const float rcut_hi = (float)sqrt(C.r_cut2) * 1.00001f;
                 for (int s2 = 0; s2 < 6; ++s2) {
                     const int r2i = (int)((rowp >> (4 * s2)) & 15u);
                     if (r2i == 15) continue;
@@ -970,9 +971,16 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
                         {
                             if (jj != 0xffffu && jj != id) {
                                 n_pairs++;
-                                const u4 q0 = philox_pair(id, jj, pid, A.k0, A.k1);
                                 const float ex = nsx - q.x, ey = nsy - q.y, ez = nsz - q.z;
                                 const float dlo = (sqrtf(fmaf(ez, ez, fmaf(ey, ey, ex * ex))) - del) * 0.999998f;
+                                // draw-free bound first: the displacement is at most the largest
+                                // Box-Muller radius of 32-bit draws (sqrt(3 * 2 ln 2^33) = 11.72)
+                                // times sqrt(2 D dt), and a partner beyond R_CUT after it is
+                                // rejected by the exact path too
+                                const float dtb = etf - q.w + dtm;
+                                const float far = dtb > 0.0f ? sqrtf(Djf2 * dtb) * 11.8f : 0.0f;
+                                if (dlo - far > rcut_hi) goto scored;
+                                const u4 q0 = philox_pair(id, jj, pid, A.k0, A.k1);
                                 // R of r_acc for U >= uf, rounded up
                                 const float uf = __uint2float_rd(q0.w) * 2.3283064365386963e-10f;
                                 const float rhi = (fmaxf(fs, __fdividef(fsc, uf)) + fadd) * 1.00002f + 1e-6f;
@@ -1007,6 +1015,7 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
                                 }
                             }
                         }
+                    scored:
                         {
                             const unsigned m = __ballot_sync(FULL, mv);
                             if (m) {
@@ -1088,11 +1097,12 @@ __global__ void k_seg_max(const unsigned long long* off, uint32_t nseg, unsigned
 // ------------------------------------------------------------------ host side
 cudaError_t irt_set_constants(const IrtConst& c) { return cudaMemcpyToSymbol(c_irt, &c, sizeof c); }
 
-static int blocks_for(const void* k, int device) {
+static int blocks_for(const void* k, int device, uint32_t limit = 0) {
     int sms = 0, per = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, IB, 0);
     if (per < 1) per = 1;
+    if (limit && (int)limit < per) per = (int)limit;
     return sms * per;
 }
 
@@ -1125,18 +1135,20 @@ __global__ void __launch_bounds__(1024) k_track_order(const uint32_t* tn, uint32
     }
 }
 
-int irt_warps(int device) { return blocks_for((const void*)k_irt_loop, device) * (IB / 32); }
+int irt_warps(int device, const IrtShape& shape) {
+    return blocks_for((const void*)k_irt_loop, device, shape.loop_per_sm) * (IB / 32);
+}
 
 // tile prefix: the scan of transport.cu
 cudaError_t launch_scan_u32(const uint32_t* cnt, uint32_t n, unsigned long long* off, cudaStream_t s);
 
-cudaError_t launch_irt(const IArgs& a, int device, cudaStream_t s, cudaEvent_t* ev) {
+cudaError_t launch_irt(const IArgs& a, int device, const IrtShape& shape, cudaStream_t s, cudaEvent_t* ev) {
     { cudaError_t me_ = cudaMemsetAsync(a.counters, 0, 4 * sizeof(uint32_t), s); if (me_ != cudaSuccess) return me_; }
     k_irt_load<<<blocks_for((const void*)k_irt_load, device), IB, 0, s>>>(a);
     cudaError_t e = launch_scan_u32(a.ttiles, a.nseg, a.toff, s);
     if (e != cudaSuccess) return e;
     if (ev) cudaEventRecord(ev[0], s);
-    k_irt_init<<<blocks_for((const void*)k_irt_init, device), IB, 0, s>>>(a);
+    k_irt_init<<<blocks_for((const void*)k_irt_init, device, shape.init_per_sm), IB, 0, s>>>(a);
     if (ev) cudaEventRecord(ev[1], s);
     k_track_order<<<1, 1024, 0, s>>>(a.tn, a.nseg, a.order);
     int sms = 0, per = 0;
@@ -1145,7 +1157,7 @@ cudaError_t launch_irt(const IArgs& a, int device, cudaStream_t s, cudaEvent_t* 
     const unsigned long long sgrid = (unsigned long long)sms * (unsigned long long)(per > 0 ? per : 1);
     k_irt_sort<<<(unsigned)(a.nseg < sgrid ? (a.nseg > 0 ? a.nseg : 1) : sgrid), SB, 0, s>>>(a);
     if (ev) cudaEventRecord(ev[2], s);
-    k_irt_loop<<<blocks_for((const void*)k_irt_loop, device), IB, 0, s>>>(a);
+    k_irt_loop<<<blocks_for((const void*)k_irt_loop, device, shape.loop_per_sm), IB, 0, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -49,9 +49,13 @@ struct IArgs {
 };
 
 cudaError_t irt_set_constants(const IrtConst& c);
-int irt_warps(int device);
-// ev (optional, 2 events): recorded after the load and after the initial pairing
-cudaError_t launch_irt(const IArgs& a, int device, cudaStream_t s, cudaEvent_t* ev = nullptr);
+// Resident blocks per SM of the pairing and event kernels: as many as fit, at
+// most the given number (0 = no limit).  The heap overflow is sized per event
+// warp, so irt_warps and launch_irt must see the same limits.
+struct IrtShape { uint32_t init_per_sm, loop_per_sm; };
+int irt_warps(int device, const IrtShape& shape);
+// ev (optional, 3 events): recorded after the load, the initial pairing and the sort
+cudaError_t launch_irt(const IArgs& a, int device, const IrtShape& shape, cudaStream_t s, cudaEvent_t* ev = nullptr);
 cudaError_t launch_group_keys(const float4* rad, unsigned long long n, unsigned long long* key, uint32_t* maxpid,
                               cudaStream_t s);
 cudaError_t launch_seg_max(const unsigned long long* off, uint32_t nseg, unsigned long long* out, cudaStream_t s);

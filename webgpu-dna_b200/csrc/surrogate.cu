@@ -45,12 +45,25 @@ __device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
     return ok != 0;
 }
 
-// wait for the phase of the given parity, at most one second
-__device__ bool mbar_wait(uint64_t* b, uint32_t parity) {
+// wait for the phase of the given parity, at most lim_ns (0: give up before
+// the first poll)
+__device__ bool mbar_wait(uint64_t* b, uint32_t parity, unsigned long long lim_ns) {
+    if (lim_ns == 0) return false;
     const unsigned long long t0 = sg_time();
     while (!mbar_try(b, parity))
-        if (sg_time() - t0 > 1000000000ull) return false;
+        if (sg_time() - t0 > lim_ns) return false;
     return true;
+}
+
+// Wait for the MMAs committed to phase `parity`.  A wait that runs out clears
+// *ok (the kernel reports SG_ERR_WAIT) and is followed by a drain wait of at
+// most WG_MMA_WAIT_NS, so that tensor memory is not read, reissued or freed
+// under an MMA still in flight.
+__device__ __forceinline__ void mma_wait(uint64_t* b, uint32_t parity, unsigned long long lim_ns, bool& ok) {
+    if (!mbar_wait(b, parity, lim_ns)) {
+        ok = false;
+        mbar_wait(b, parity, WG_MMA_WAIT_NS);
+    }
 }
 
 __device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols) {     // one full warp
@@ -166,7 +179,11 @@ __global__ void __launch_bounds__(SG_TILE, 1) k_sg_fwd(SgFwdArgs a) {
     for (int c = 0; c < SG_IN / 8; ++c) {
         __align__(16) __nv_bfloat16 h[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) h[j] = __float2bfloat16_rn(live ? a.X[(size_t)src * SG_IN + 8 * c + j] : 0.0f);
+        for (int j = 0; j < 8; ++j) {
+            float x = live ? a.X[(size_t)src * SG_IN + 8 * c + j] : 0.0f;
+            if (a.xmean && live) x = (x - a.xmean[8 * c + j]) * a.xinv[8 * c + j];
+            h[j] = __float2bfloat16_rn(x);
+        }
         *reinterpret_cast<uint4*>(bufA + coff(tid, 8 * c, SG_IN)) = *reinterpret_cast<uint4*>(h);
         if (a.H0 && live) *reinterpret_cast<uint4*>(a.H0 + (size_t)r * SG_IN + 8 * c) = *reinterpret_cast<uint4*>(h);
     }
@@ -182,7 +199,7 @@ __global__ void __launch_bounds__(SG_TILE, 1) k_sg_fwd(SgFwdArgs a) {
             gemm_issue(tm, s2u(bufA), s2u(bufB), SG_TILE, N, K);
             umma_commit(&bar);
         }
-        ok = mbar_wait(&bar, (uint32_t)(l & 1)) && ok;
+        mma_wait(&bar, (uint32_t)(l & 1), (l == 0 && a.give_up_first) ? 0ull : a.mma_ns, ok);
         tc_after_sync();
         const float* bias = a.w.p + (l == 0 ? SG_OFF_B1 : l == 1 ? SG_OFF_B2 : l == 2 ? SG_OFF_B3 : SG_OFF_B4);
         float* Zs = l == 0 ? a.Z1 : l == 1 ? a.Z2 : l == 2 ? a.Z3 : nullptr;
@@ -191,8 +208,28 @@ __global__ void __launch_bounds__(SG_TILE, 1) k_sg_fwd(SgFwdArgs a) {
             float v[32];
             tmem_ld32(lane_tm + (uint32_t)c0, v);
             if (l == 3) {
-                if (live)
+                if (live && a.Y)
                     for (int j = 0; j < 32 && c0 + j < N; ++j) a.Y[(size_t)r * SG_OUT + c0 + j] = v[j] + bias[c0 + j];
+                if (a.acc) {
+                    // column sums over the tile's rows: each warp reduces its 32
+                    // rows, lane 0 adds the warp's partial in f64
+                    const float e = live ? (a.E ? a.E[r] : a.E0) : 0.0f;
+#pragma unroll 4
+                    for (int j = 0; j < 32; ++j) {
+                        const int col = c0 + j;
+                        if (col >= N) break;
+                        float w = live ? ((v[j] + bias[col]) * a.ystd[col] + a.ymean[col]) * e : 0.0f;
+#pragma unroll
+                        for (int o = 16; o; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+                        if ((tid & 31) == 0) atomicAdd(&a.acc[col], (double)w);
+                    }
+                    if (c0 == 0) {
+                        float w = e;
+#pragma unroll
+                        for (int o = 16; o; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+                        if ((tid & 31) == 0) atomicAdd(&a.acc[SG_OUT], (double)w);
+                    }
+                }
                 continue;
             }
 #pragma unroll
@@ -293,7 +330,7 @@ __global__ void __launch_bounds__(SG_TILE, 1) k_sg_bwd(SgBwdArgs a) {
             if (l > 0) gemm_issue(tm, s2u(bufG), s2u(bufW), SG_TILE, n_in, n_out);              // dH
             umma_commit(&bar);
         }
-        ok = mbar_wait(&bar, (uint32_t)((3 - l) & 1)) && ok;
+        mma_wait(&bar, (uint32_t)((3 - l) & 1), (l == 3 && a.give_up_first) ? 0ull : a.mma_ns, ok);
         tc_after_sync();
         // weight gradient: TMEM row tid of D_dW
         const int woff = l == 0 ? SG_OFF_W1 : l == 1 ? SG_OFF_W2 : l == 2 ? SG_OFF_W3 : SG_OFF_W4;

@@ -32,6 +32,16 @@ struct SgFwdArgs {
     __nv_bfloat16 *H0, *H1, *H2, *H3;
     float *Z1, *Z2, *Z3;
     uint32_t* err;
+    unsigned long long mma_ns;               // bound of a tensor-core wait
+    uint32_t give_up_first;                  // test switch: a tile's first wait gives up at once
+    // optional fusions of the chemistry path: standardise X on load
+    // ((x - xmean) * xinv), and add the energy-weighted de-standardised outputs
+    // ((y * ystd + ymean) * E_track, then E_track) to acc[0..80] (Y may be null)
+    const float *xmean, *xinv;
+    const float *ymean, *ystd;
+    const float* E;                          // per-row energy, or null for E0
+    float E0;
+    double* acc;
 };
 
 struct SgBwdArgs {
@@ -45,6 +55,8 @@ struct SgBwdArgs {
     float* grad;                             // f32, SG_NPARAM, accumulated with atomics
     double* loss;                            // sum of squared errors
     uint32_t* err;
+    unsigned long long mma_ns;
+    uint32_t give_up_first;
 };
 
 // descriptors of the tracks of a canonical rad_buf

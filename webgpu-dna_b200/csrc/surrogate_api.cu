@@ -34,6 +34,10 @@ struct SgState {
     float *desc = nullptr, *xs = nullptr, *pred = nullptr;
     uint64_t desc_n = 0, desc_cap = 0;
     double* acc = nullptr;
+    // bound of the kernels' tensor-core waits and the test switch (from the context)
+    unsigned long long mma_ns = WG_MMA_WAIT_NS;
+    uint32_t give_up_first = 0;
+    cudaEvent_t ev[2] = {nullptr, nullptr};   // timing of wgdna_surrogate_chemistry
 };
 
 void sg_free(SgState* s) {
@@ -42,6 +46,7 @@ void sg_free(SgState* s) {
                     s->rows, s->Y, s->H0, s->H1, s->H2, s->H3, s->Z1, s->Z2, s->Z3, s->loss, s->err,
                     s->desc, s->xs, s->pred, s->acc};
     for (void* q : ptrs) if (q) cudaFree(q);
+    for (cudaEvent_t e : s->ev) if (e) cudaEventDestroy(e);
     delete s;
 }
 
@@ -73,9 +78,16 @@ double u01(uint64_t& s) { return (double)(smix(s) >> 11) * (1.0 / 90071992547409
 int ensure_state(wgdna_ctx* c, CtxView& v, SgState** out) {
     ctx_view(c, &v);
     WG_CUDA_OK(cudaSetDevice(v.device));
-    if (*v.sg) { *out = *v.sg; return WGDNA_OK; }
+    if (*v.sg) {
+        (*v.sg)->mma_ns = v.mma_ns;
+        (*v.sg)->give_up_first = v.mma_give_up_first ? 1u : 0u;
+        *out = *v.sg;
+        return WGDNA_OK;
+    }
     SgState* s = new SgState();
     *v.sg = s;
+    s->mma_ns = v.mma_ns;
+    s->give_up_first = v.mma_give_up_first ? 1u : 0u;
     STRY(salloc(&s->p, SG_NPARAM)); STRY(salloc(&s->m, SG_NPARAM)); STRY(salloc(&s->v, SG_NPARAM));
     STRY(salloc(&s->g, SG_NPARAM));
     STRY(salloc(&s->W, SG_WTOTAL)); STRY(salloc(&s->WT, SG_WTOTAL));
@@ -135,12 +147,12 @@ int fwd_bwd(SgState* s, cudaStream_t st, const uint32_t* d_rows, uint32_t n) {
     SgFwdArgs f{};
     f.X = s->X; f.rows = d_rows; f.n = n; f.w = weights(s); f.Y = s->Y;
     f.H0 = s->H0; f.H1 = s->H1; f.H2 = s->H2; f.H3 = s->H3; f.Z1 = s->Z1; f.Z2 = s->Z2; f.Z3 = s->Z3;
-    f.err = s->err;
+    f.err = s->err; f.mma_ns = s->mma_ns; f.give_up_first = s->give_up_first;
     WG_CUDA_OK(launch_sg_forward(f, st));
     SgBwdArgs b{};
     b.T = s->T; b.rows = d_rows; b.n = n; b.w = f.w; b.Y = s->Y;
     b.H0 = s->H0; b.H1 = s->H1; b.H2 = s->H2; b.H3 = s->H3; b.Z1 = s->Z1; b.Z2 = s->Z2; b.Z3 = s->Z3;
-    b.grad = s->g; b.loss = s->loss; b.err = s->err;
+    b.grad = s->g; b.loss = s->loss; b.err = s->err; b.mma_ns = s->mma_ns; b.give_up_first = s->give_up_first;
     WG_CUDA_OK(launch_sg_backward(b, st));
     return WGDNA_OK;
 }
@@ -317,6 +329,7 @@ extern "C" int wgdna_surrogate_predict(wgdna_ctx* c, const float* X, uint64_t n,
     WG_CUDA_OK(launch_sg_standardise(src, s->xs, n, SG_IN, s->xmean, s->xinv, v.stream));
     SgFwdArgs f{};
     f.X = s->xs; f.n = (uint32_t)n; f.w = weights(s); f.Y = s->pred; f.err = s->err;
+    f.mma_ns = s->mma_ns; f.give_up_first = s->give_up_first;
     WG_CUDA_OK(launch_sg_forward(f, v.stream));
     STRY(check_err(s, v.stream, "wgdna_surrogate_predict"));
     if (G) {
@@ -353,24 +366,48 @@ extern "C" int wgdna_track_descriptors(wgdna_ctx* c, float* out, uint64_t cap, u
 }
 
 // the surrogate's G(t) for all tracks of the last transport, energy-weighted
-// like the IRT's (counts over n_therm * E / 100): G[16][5]
+// like the IRT's (counts over n_therm * E / 100): G[16][5].  Three launches
+// and one host synchronisation: the descriptors, the forward pass (inputs
+// standardised on load, the energy-weighted sums of its de-standardised
+// outputs added in its last epilogue), and the read-back of those sums.
 extern "C" int wgdna_surrogate_chemistry(wgdna_ctx* c, double* G, float* ms) {
     if (!c || !G) { wg_set_error("wgdna_surrogate_chemistry: NULL argument"); return WGDNA_ERR_ARG; }
     CtxView v;
     SgState* s;
     STRY(ensure_state(c, v, &s));
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0); cudaEventCreate(&e1);
-    cudaEventRecord(e0, v.stream);
-    STRY(wgdna_track_descriptors(c, nullptr, 0, nullptr));
-    STRY(wgdna_surrogate_predict(c, nullptr, 0, nullptr));
-    WG_CUDA_OK(launch_sg_reduce(s->pred, (uint32_t)s->desc_n, s->ymean, s->ystd, v.Eprim, v.E0, s->acc, v.stream));
-    cudaEventRecord(e1, v.stream);
+    if (!v.have_transport) { wg_set_error("wgdna_surrogate_chemistry: no transport result in the context"); return WGDNA_ERR_STATE; }
+    const uint64_t n = v.nseg;
+    if (n > s->desc_cap) {
+        STRY(salloc(&s->desc, n * SG_IN)); STRY(salloc(&s->xs, n * SG_IN)); STRY(salloc(&s->pred, n * SG_OUT));
+        s->desc_cap = n;
+    }
+    if (!s->ev[0]) {
+        WG_CUDA_OK(cudaEventCreate(&s->ev[0]));
+        WG_CUDA_OK(cudaEventCreate(&s->ev[1]));
+    }
+    WG_CUDA_OK(cudaEventRecord(s->ev[0], v.stream));
+    WG_CUDA_OK(cudaMemsetAsync(s->acc, 0, (SG_OUT + 1) * sizeof(double), v.stream));
+    DescArgs da{v.rad, v.seg_off, v.nseg, v.Eprim, v.E0, s->desc};
+    WG_CUDA_OK(launch_descriptors(da, v.stream));
+    s->desc_n = n;
+    SgFwdArgs f{};
+    f.X = s->desc; f.n = (uint32_t)n; f.w = weights(s); f.Y = nullptr; f.err = s->err;
+    f.mma_ns = s->mma_ns; f.give_up_first = s->give_up_first;
+    f.xmean = s->xmean; f.xinv = s->xinv; f.ymean = s->ymean; f.ystd = s->ystd;
+    f.E = v.Eprim; f.E0 = v.E0; f.acc = s->acc;
+    WG_CUDA_OK(launch_sg_forward(f, v.stream));
+    WG_CUDA_OK(cudaEventRecord(s->ev[1], v.stream));
     double acc[SG_OUT + 1];
+    uint32_t err = 0;
     WG_CUDA_OK(cudaMemcpyAsync(acc, s->acc, sizeof acc, cudaMemcpyDeviceToHost, v.stream));
+    WG_CUDA_OK(cudaMemcpyAsync(&err, s->err, 4, cudaMemcpyDeviceToHost, v.stream));
     WG_CUDA_OK(cudaStreamSynchronize(v.stream));
-    if (ms) cudaEventElapsedTime(ms, e0, e1);
-    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    if (err) {
+        wg_set_error("wgdna_surrogate_chemistry: device error flags 0x%x", err);
+        cudaMemsetAsync(s->err, 0, 4, v.stream);
+        return WGDNA_ERR_DEVICE;
+    }
+    if (ms) cudaEventElapsedTime(ms, s->ev[0], s->ev[1]);
     for (int k = 0; k < SG_OUT; ++k) G[k] = acc[SG_OUT] > 0 ? acc[k] / acc[SG_OUT] : 0.0;
     return WGDNA_OK;
 }

@@ -19,6 +19,8 @@ struct CtxView {
     const float* Eprim;                  // per-primary energies of that transport, or null
     float E0;                            // its energy otherwise
     SgState** sg;
+    unsigned long long mma_ns;           // bound of a surrogate kernel's tensor-core wait
+    bool mma_give_up_first;              // test switch: the first wait of a tile gives up at once
 };
 
 void sg_free(SgState* s);

@@ -29,12 +29,7 @@ constexpr int TB = 256;            // threads per block
 constexpr int TW = TB / 32;        // warps per block
 constexpr int STG = 192;           // staged rad entries per warp
 constexpr int STG_FLUSH = 96;      // 32 lanes x at most 3 entries per step
-constexpr uint32_t PRIM_TAKE = 2;  // primaries a warp may start per iteration
-constexpr int STASH = 48;          // secondaries a warp keeps in shared memory
-constexpr int STASH_KEEP = 16;     // kept when a full stash spills to the global queue
-constexpr int STASH_SPILL = 32;
-constexpr unsigned long long IDLE_LIMIT_NS = 30000000000ull;   // 30 s without work
-constexpr unsigned long long READY_LIMIT_NS = 2000000000ull;   // 2 s for a queued record
+constexpr int STASH = (int)TRANSPORT_STASH;   // secondaries a warp keeps in shared memory
 
 __device__ __forceinline__ unsigned long long gtime() {
     unsigned long long t;
@@ -317,7 +312,7 @@ __device__ void push_global(const TArgs& A, const StashRec* r, int n, int lane_s
         rec->meta.x = r[k].pid;
         rec->meta.y = r[k].sub;
         __threadfence();
-        *(volatile uint32_t*)&rec->meta.z = A.epoch;     // publish
+        *(volatile uint32_t*)&rec->meta.z = A.pub_epoch;     // publish
     }
 }
 
@@ -429,7 +424,7 @@ __device__ __forceinline__ void interact(const TArgs& A, Blk& b, Particle& q, De
                         if (pfl > 1e-10f) { q.dx = pfx / pfl; q.dy = pfy / pfl; q.dz = pfz / pfl; }
                         if (q.nsec >= (1u << 17)) atomicOr(&A.st->err, DERR_KEY_RANGE);
                         StashRec r{px, py, pz, W_sec, sdx, sdy, sdz, q.pid, q.nsec};
-                        int slot = atomicAdd(b.stn, 1);
+                        int slot = A.stash_spill ? atomicAdd(b.stn, 1) : STASH;
                         if (slot < STASH) b.stash[slot] = r;
                         else push_global(A, &r, 1, 0);
                     }
@@ -766,7 +761,7 @@ __global__ void __launch_bounds__(TB, 2) k_transport(TArgs A) {
             }
         }
         const bool idle_warp = need == 0xffffffffu;
-        const bool poll = idle_warp || (it & 7u) == 0u;
+        const bool poll = idle_warp || (it & A.poll_mask) == 0u;
         // 2) the global queue
         if (need && poll) {
             uint32_t base = 0, got = 0;
@@ -788,8 +783,14 @@ __global__ void __launch_bounds__(TB, 2) k_transport(TArgs A) {
                 const SecRec* rec = A.secq + base + rank;
                 unsigned long long t0 = gtime();
                 bool ok = true;
+                // bounded wait for the record's publication; once one wait has
+                // run out the run is failed and no lane waits again
                 while (*(volatile const uint32_t*)&rec->meta.z != A.epoch) {
-                    if (gtime() - t0 > READY_LIMIT_NS) { atomicOr(&S->err, DERR_QUEUE_WAIT); ok = false; break; }
+                    if ((*(volatile uint32_t*)&S->err & DERR_QUEUE_WAIT) || gtime() - t0 > A.ready_ns) {
+                        atomicOr(&S->err, DERR_QUEUE_WAIT);
+                        ok = false;
+                        break;
+                    }
                     __nanosleep(64);
                 }
                 __threadfence();
@@ -807,7 +808,7 @@ __global__ void __launch_bounds__(TB, 2) k_transport(TArgs A) {
         if (need && poll && *(volatile uint32_t*)&S->prim_next.v < A.np) {
             uint32_t pb = 0, pg = 0;
             if (lane == 0) {
-                uint32_t take = min((uint32_t)__popc(need), PRIM_TAKE);
+                uint32_t take = min((uint32_t)__popc(need), A.prim_take);
                 uint32_t old = atomicAdd(&S->prim_next.v, take);
                 if (old < A.np) { pg = min(take, A.np - old); pb = old; }
             }
@@ -830,7 +831,7 @@ __global__ void __launch_bounds__(TB, 2) k_transport(TArgs A) {
             done = __shfl_sync(0xffffffffu, done, 0);
             if (done) break;
             if (idle_since == 0) idle_since = gtime();
-            if (gtime() - idle_since > IDLE_LIMIT_NS) { if (lane == 0) atomicOr(&S->err, DERR_IDLE_WAIT); break; }
+            if (gtime() - idle_since > A.idle_ns) { if (lane == 0) atomicOr(&S->err, DERR_IDLE_WAIT); break; }
             __nanosleep(sleep_ns);
             sleep_ns = min(sleep_ns * 2, 8192u);
             continue;
@@ -843,9 +844,9 @@ __global__ void __launch_bounds__(TB, 2) k_transport(TArgs A) {
         if (lane == 0) {
             int sn = *b.stn;
             if (sn > STASH) sn = STASH;
-            if (sn >= STASH_SPILL) {
-                push_global(A, b.stash + STASH_KEEP, sn - STASH_KEEP, 0);
-                sn = STASH_KEEP;
+            if (A.stash_spill && sn >= (int)A.stash_spill) {
+                push_global(A, b.stash + A.stash_keep, sn - (int)A.stash_keep, 0);
+                sn = (int)A.stash_keep;
             }
             *b.stn = sn;
         }
@@ -969,7 +970,7 @@ size_t transport_smem_bytes() {
 
 // resident CTAs of k_transport on `device` (the current device); the shared
 // memory attribute is set on each device the first time
-int transport_blocks(int device) {
+int transport_blocks(int device, uint32_t ctas_per_sm) {
     static DeviceOnce attr;
     attr.run([] {
         return cudaFuncSetAttribute(k_transport, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -979,6 +980,7 @@ int transport_blocks(int device) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_transport, TB, transport_smem_bytes());
     if (per < 1) per = 1;
+    if (ctas_per_sm && (int)ctas_per_sm < per) per = (int)ctas_per_sm;
     return sms * per;
 }
 

@@ -13,6 +13,8 @@ LIB_PATH = os.path.join(PKG_ROOT, "libwgdna.so")
 TABLES_PATH = os.path.join(PKG_ROOT, "data", "cross_sections.bin")
 
 WGDNA_OK = 0
+WGDNA_ERR_ARG, WGDNA_ERR_CUDA, WGDNA_ERR_TABLES, WGDNA_ERR_CAPACITY = -1, -2, -3, -4
+WGDNA_ERR_DEVICE, WGDNA_ERR_NOMEM, WGDNA_ERR_STATE = -5, -6, -7
 ERRORS = {-1: "WGDNA_ERR_ARG", -2: "WGDNA_ERR_CUDA", -3: "WGDNA_ERR_TABLES", -4: "WGDNA_ERR_CAPACITY",
           -5: "WGDNA_ERR_DEVICE", -6: "WGDNA_ERR_NOMEM", -7: "WGDNA_ERR_STATE"}
 
@@ -26,8 +28,11 @@ EXPORTS = ["wgdna_default_cfg", "wgdna_create", "wgdna_destroy", "wgdna_last_err
            "wgdna_surrogate_load", "wgdna_surrogate_train", "wgdna_surrogate_grad", "wgdna_surrogate_predict",
            "wgdna_surrogate_chemistry", "wgdna_dose_sum", "wgdna_dose_projection", "wgdna_score_voxel_ssb",
            "wgdna_expected_dsb_local", "wgdna_chem_grid", "wgdna_device_views", "wgdna_score_draws",
-           "wgdna_cluster_device"]
+           "wgdna_cluster_device", "wgdna_set_wait_limits", "wgdna_default_tuning", "wgdna_get_tuning",
+           "wgdna_set_tuning"]
 SG_IN, SG_OUT, SG_NPARAM = 64, 80, 51664
+# test switches of wgdna_set_wait_limits
+WGDNA_TEST_UNPUBLISHED, WGDNA_TEST_MMA_WAIT = 1, 2
 
 
 class WgdnaError(RuntimeError):
@@ -39,6 +44,16 @@ class WgdnaError(RuntimeError):
 class Cfg(C.Structure):
     _fields_ = [("device", C.c_int), ("tables_path", C.c_char_p), ("max_primaries", C.c_uint32),
                 ("max_sec", C.c_uint32), ("max_rad", C.c_uint64), ("vc", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class Tuning(C.Structure):
+    """wgdna_tuning: launch and scheduling shapes (results never depend on them)."""
+    _fields_ = [("transport_ctas_per_sm", C.c_uint32), ("prim_take", C.c_uint32), ("stash_keep", C.c_uint32),
+                ("stash_spill", C.c_uint32), ("queue_poll", C.c_uint32), ("irt_init_blocks_per_sm", C.c_uint32),
+                ("irt_loop_blocks_per_sm", C.c_uint32)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
 
 
 class TransportParams(C.Structure):
@@ -149,6 +164,10 @@ def lib():
         "wgdna_device_views": (C.c_int, [vp, P(DeviceView)]),
         "wgdna_score_draws": (C.c_int, [vp, C.c_uint32, P(SsbResult)]),
         "wgdna_cluster_device": (C.c_int, [vp, P(DsbResult)]),
+        "wgdna_set_wait_limits": (C.c_int, [vp, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint32]),
+        "wgdna_default_tuning": (None, [P(Tuning)]),
+        "wgdna_get_tuning": (C.c_int, [vp, P(Tuning)]),
+        "wgdna_set_tuning": (C.c_int, [vp, P(Tuning)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -209,6 +228,19 @@ class Context:
 
     def set_stream(self, stream_ptr):
         check("wgdna_set_stream", lib().wgdna_set_stream(self.h, C.c_void_p(stream_ptr or 0)))
+
+    def tuning(self):
+        t = Tuning()
+        check("wgdna_get_tuning", lib().wgdna_get_tuning(self.h, C.byref(t)))
+        return t
+
+    def set_tuning(self, t=None, **fields):
+        """Apply a Tuning (or the current one with ``fields`` changed)."""
+        t = t if t is not None else self.tuning()
+        for k, v in fields.items():
+            setattr(t, k, int(v))
+        check("wgdna_set_tuning", lib().wgdna_set_tuning(self.h, C.byref(t)))
+        return t
 
 
 def reaction_table():

@@ -9,6 +9,7 @@ track's energy / 100 eV.  The IRT stays the reference: ``chemistry`` falls back
 to it when a batch's descriptors leave the training range.
 """
 import ctypes as C
+import time
 
 import numpy as np
 
@@ -120,3 +121,49 @@ def chemistry(ctx, n_therm, E_eV, seed=1):
     finally:
         L.wgdna_irt_record_curves(ctx.h, 0)
     return cv.sum(axis=0) / (n_therm * E_eV / 100.0), False
+
+
+TRAIN_ENERGIES = (1000.0, 3000.0, 10000.0)
+TRAIN_SCHEDULE = ((60, 2e-3), (30, 5e-4), (15, 1e-4))
+
+
+def train_on_irt(ctx, batches_per_energy=8, energies=TRAIN_ENERGIES, seed0=100, schedule=TRAIN_SCHEDULE):
+    """The training recipe: IRT curves of batches_per_energy x 4096 tracks at
+    each energy (transport seeds seed0, seed0 + 7, ...), then the staged Adam
+    fit on the device.  Returns a summary of the run."""
+    Xs, Gs = [], []
+    seed = seed0
+    t0 = time.perf_counter()
+    for E in energies:
+        for _ in range(batches_per_energy):
+            X, G, _, _ = track_data(ctx, np.full(4096, E, np.float32), seed)
+            seed += 7
+            Xs.append(X)
+            Gs.append(G)
+    X, G = np.concatenate(Xs), np.concatenate(Gs)
+    t1 = time.perf_counter()
+    losses = fit(ctx, X, G, schedule=schedule, seed=1)
+    return {"tracks": int(X.shape[0]), "data_s": t1 - t0, "train_s": time.perf_counter() - t1,
+            "loss_first": float(losses[0]), "loss_last": float(losses[-1]), "epochs": int(losses.size)}
+
+
+def g_errors(gi, gp):
+    """Largest relative error of a batch G (16 x 5) at 1 us and over every
+    time and species where the IRT's G exceeds 0.05."""
+    rel = np.abs(gp - gi) / np.maximum(np.abs(gi), 1e-12)
+    return float(rel[15].max()), float(rel[gi > 0.05].max())
+
+
+def held_out(ctx, E, seed):
+    """One held-out 4096-track batch at energy E: the IRT's batch G(t) from its
+    per-track curves, the plain batched IRT's device time, the surrogate
+    chemistry's batch G(t) and device time, on the same tracks."""
+    L = _lib.lib()
+    Xh, Gh, Eh, _ = track_data(ctx, np.full(4096, E, np.float32), seed)
+    gi = batch_G(Gh, Eh)
+    ir = _lib.IrtResult()
+    _lib.check("wgdna_irt", L.wgdna_irt(ctx.h, int(Eh.size), float(E), 1, C.byref(ir)))
+    Gc = np.zeros(80)
+    ms = C.c_float()
+    _lib.check("wgdna_surrogate_chemistry", L.wgdna_surrogate_chemistry(ctx.h, _lib.ptr(Gc), C.byref(ms)))
+    return gi, Gc.reshape(16, 5), float(ir.ms), float(ms.value), Xh
