@@ -357,6 +357,14 @@ def run_native(args, ws, rank, local):
     # the second half of the metric: the learned chemistry against the IRT
     # (trained in this run by the library's kernels; untimed by the step clock)
     surrogate = surrogate_block(ctx, 3, 1) if ws == 1 and not args.no_surrogate else None
+    # the other workloads of the benchmark table, untimed by the step clock:
+    # one synthetic track (C1), mixed energies (C3), the DNA-damage sweep (C5,
+    # on the network the surrogate block trained)
+    workloads = None
+    if ws == 1 and not args.no_workloads:
+        workloads = {"track": track_block(), "mixed": mixed_block()}
+        if surrogate is not None:
+            workloads["sweep"] = sweep_block(ctx, args.sweep_n)
 
     # roofline of the dominant kernel: algorithmic bytes per launch / its mean duration
     pk = peaks()
@@ -414,6 +422,7 @@ def run_native(args, ws, rank, local):
             "clocks": clocks,
             "physics": physics,
             "surrogate": surrogate,
+            "workloads": workloads,
             "job": {"ssb": job.get("ssb"), "dsb": job.get("dsb"), "in_reach": job.get("reach")} if ws > 1 else None,
             "work": {"rad_n": int(R), "sec_n": int(S), "steps": int(st.steps), "irt_pairs": int(ir.n_pairs),
                      "irt_events": int(ir.n_events), "irt_init_events": int(Ei), "irt_species": int(Np),
@@ -671,6 +680,96 @@ def run_mixed(args):
     ctx.close()
 
 
+def track_block(steps=5, warmup=2):
+    """C1 in the default line: one synthetic 10 keV-like track (510 spurs x 6
+    species on a 2.7 um walk) through the IRT to 1 us from pinned host memory;
+    device ms per track and the oracle's one-thread time on the same track."""
+    import ctypes as C
+    import torch
+    import oracle
+    import wgdna
+    from wgdna import _lib, synthetic
+    L = _lib.lib()
+    ctx = wgdna.Context(max_primaries=16, max_rad=1_000_000, max_sec=100_000)
+    try:
+        rad = synthetic.synthetic_track()
+        rad_h = torch.from_numpy(rad).pin_memory()
+        ir = _lib.IrtResult()
+        ms = []
+        for k in range(warmup + steps):
+            _lib.check("wgdna_run_irt", L.wgdna_run_irt(ctx.h, C.c_void_p(rad_h.data_ptr()), rad.shape[0], 1, 1e4, 1,
+                                                        C.byref(ir)))
+            if k >= warmup:
+                ms.append(ir.ms)
+        t0 = time.perf_counter()
+        oracle.irt(rad, 1, 1e4, seed=1, nthreads=1)
+        cpu_s = time.perf_counter() - t0
+        m = sum(ms) / len(ms)
+        return {"workload": "one synthetic track, 510 spurs x 6 species (2550 tracked) on a 2.7 um walk, IRT to 1 us",
+                "ms_per_track": round(m, 4), "tracks_per_s": round(1000.0 / m, 2), "pairs": int(ir.n_pairs),
+                "events": int(ir.n_events), "reacted": int(ir.n_reacted),
+                "cpu_one_thread_s": round(cpu_s, 4), "speedup_vs_one_thread": round(cpu_s * 1000.0 / m, 1)}
+    finally:
+        ctx.close()
+
+
+def mixed_block(steps=2, warmup=1, seed=0):
+    """C3 in the default line: 65,536 primaries, E log-uniform 100 eV - 30 keV,
+    one transport launch, the IRT over all tracks; then the IRT alone on each
+    species-count bucket's tracks (pairs per second per bucket)."""
+    import ctypes as C
+    import numpy as np
+    import torch
+    import wgdna
+    from wgdna import _lib, synthetic
+    L = _lib.lib()
+    N = MIXED_N
+    E = synthetic.mixed_energies(N)
+    ctx = wgdna.Context(max_primaries=N, max_rad=max(N * 1100, 1_000_000), max_sec=max(N * 130, 100_000))
+    try:
+        E_h = torch.from_numpy(E).pin_memory()
+        p = wgdna.transport_params(N, 10000.0, 15000.0, 7.5, seed=seed, dna_enable=0)
+        p.E_per_primary = E_h.data_ptr()
+        st, ir = _lib.TransportStats(), _lib.IrtResult()
+        Emean = float(np.mean(E.astype(np.float64)))
+        tr, pa, ev, tot = [], [], [], []
+        for k in range(warmup + steps):
+            _lib.check("wgdna_transport", L.wgdna_transport(ctx.h, C.byref(p), C.byref(st)))
+            _lib.check("wgdna_irt", L.wgdna_irt(ctx.h, st.n_therm, Emean, seed + 1, C.byref(ir)))
+            if k >= warmup:
+                tr.append(st.ms_transport)
+                pa.append(ir.ms)
+                tot.append(st.ms_transport + st.ms_canon + ir.ms)
+        rad = np.empty(st.rad_n_stored * 4, np.float32)
+        rn = C.c_uint64()
+        _lib.check("copy_out", L.wgdna_transport_copy_out(ctx.h, None, None, _lib.ptr(rad), st.rad_n_stored,
+                                                           C.byref(rn)))
+        rad = rad[:4 * min(rn.value, st.rad_n_stored)].reshape(-1, 4)
+        w = rad[:, 3].astype(np.int64)
+        pid, code = w >> 3, w & 7
+        tracked = np.bincount(pid[code != 7], minlength=N)
+        buckets = []
+        irb = _lib.IrtResult()
+        edges = (1, 100, 500, 1000, 2000, 5000, 1 << 30)
+        for lo, hi in zip(edges[:-1], edges[1:]):
+            sel = np.nonzero((tracked >= lo) & (tracked < hi))[0]
+            if sel.size == 0:
+                continue
+            sub = np.ascontiguousarray(rad[np.isin(pid, sel)])
+            _lib.check("wgdna_run_irt", L.wgdna_run_irt(ctx.h, _lib.ptr(sub), sub.shape[0], int(sel.size), Emean,
+                                                        seed + 1, C.byref(irb)))
+            buckets.append({"species": f"{lo}-{hi - 1}" if hi < (1 << 30) else f">={lo}", "tracks": int(sel.size),
+                            "irt_ms": round(irb.ms, 3), "pairs_per_s": irb.n_pairs / (irb.ms / 1000.0)})
+        m = sum(tot) / len(tot)
+        return {"workload": f"{N} primaries, E log-uniform 100 eV - 30 keV, one transport launch, IRT to 1 us "
+                            "over all tracks",
+                "primaries_per_s": round(N / (m / 1000.0), 1), "ms_per_step": round(m, 3),
+                "transport_ms": round(sum(tr) / len(tr), 3), "irt_ms": round(sum(pa) / len(pa), 3),
+                "tracks": int(ir.n_tracks), "irt_species": int(ir.n_particles), "irt_buckets": buckets}
+    finally:
+        ctx.close()
+
+
 SURROGATE_ENERGIES = (1000.0, 3000.0, 10000.0)
 
 
@@ -746,79 +845,95 @@ def run_surrogate(args):
     ctx.close()
 
 
-def run_sweep(args):
-    """DNA-damage sweep: primaries at 1, 3 and 10 keV in batches of 4096
-    through transport, the surrogate chemistry (the IRT checking 1 % of the
-    batches) and direct SSB + DSB scoring (10 bp window) on the 21 x 21 fibre
-    grid; yields per Gy and per primary."""
+def sweep_block(ctx, n_per=1_000_000, B=4096, energies=(1000.0, 3000.0, 10000.0)):
+    """C5: n_per primaries at each energy in batches of B through transport,
+    the surrogate chemistry (the context's trained network; the IRT checks 1 %
+    of the batches) and direct SSB + DSB scoring (10 bp window) on the 21 x 21
+    fibre grid; yields per Gy and per primary, device and wall throughput."""
     import ctypes as C
     import numpy as np
     import wgdna
-    from wgdna import _lib, surrogate as S
+    from wgdna import _lib
     L = _lib.lib()
-    n_per = args.np if args.np != NP else 1_000_000
-    B = 4096
-    ctx = wgdna.Context(max_primaries=B, max_rad=8_000_000, max_sec=1_200_000)
-    train = S.train_on_irt(ctx, 8)
     dna = wgdna.build_dna_target()
     box = 15000.0
     mass_kg = ((2 * box * 1e-9) ** 3) * 1000.0
     rows = {}
-    stream_ms = 0.0
+    stream_ms = wall_all = 0.0
+    for E in energies:
+        nb = (n_per + B - 1) // B
+        st, ssb, dsb = _lib.TransportStats(), _lib.SsbResult(), _lib.DsbResult()
+        ir = _lib.IrtResult()
+        dep = 0.0
+        n_ssb = n_dsb = 0
+        checks = []
+        Gsum = np.zeros(80)
+        ms_tr = ms_sg = ms_sc = 0.0
+        t0 = time.perf_counter()
+        for b in range(nb):
+            n = min(B, n_per - b * B)
+            p = wgdna.transport_params(n, E, box, 7.5, dna=dna, seed=int(E) * 1000 + b, dna_enable=1)
+            p.pid_base = b * B
+            _lib.check("transport", L.wgdna_transport(ctx.h, C.byref(p), C.byref(st)))
+            Gc = np.zeros(80)
+            ms = C.c_float()
+            _lib.check("chem", L.wgdna_surrogate_chemistry(ctx.h, _lib.ptr(Gc), C.byref(ms)))
+            if b % 100 == 50 or nb < 100 and b == nb // 2:                      # the IRT checks 1 %
+                L.wgdna_irt_record_curves(ctx.h, 1)
+                _lib.check("irt", L.wgdna_irt(ctx.h, st.n_therm, E, b + 1, C.byref(ir)))
+                L.wgdna_irt_record_curves(ctx.h, 0)
+                # 1 ps, 100 ps, 10 ns and 1 us are both IRT checkpoints and curve times
+                gi = np.array(ir.G)[[0, 2, 4, 6]]
+                gs = Gc.reshape(16, 5)[[0, 5, 10, 15]]
+                checks.append(float((np.abs(gs - gi) / np.maximum(gi, 1e-12))[gi > 0.05].max()))
+            _lib.check("score", L.wgdna_score(ctx.h, 0x12345678, C.byref(ssb), C.byref(dsb)))
+            dep += st.dep_eV_f64
+            n_ssb += ssb.ssb
+            n_dsb += dsb.dsb
+            Gsum += Gc * n * E
+            ms_tr += st.ms_transport
+            ms_sg += ms.value
+            ms_sc += ssb.ms + dsb.ms
+        wall = time.perf_counter() - t0
+        dose = dep * 1.602e-19 / mass_kg
+        gbp = dna.n_bp * 1e-9
+        rows[int(E)] = {"primaries": n_per, "batches": nb, "dose_Gy": dose,
+                        "SSB_per_primary": n_ssb / n_per, "DSB_per_primary": n_dsb / n_per,
+                        "DSB_per_Gy_Gbp": n_dsb / (dose * gbp) if dose > 0 else 0.0,
+                        "SSB_per_Gy_Gbp": n_ssb / (dose * gbp) if dose > 0 else 0.0,
+                        "G_1us": [round(float(v), 4) for v in (Gsum / (n_per * E)).reshape(16, 5)[15]],
+                        "irt_check_max_rel_err": max(checks) if checks else None, "irt_checked_batches": len(checks),
+                        "device_ms": {"transport": round(ms_tr, 2), "surrogate": round(ms_sg, 2),
+                                      "scoring": round(ms_sc, 2)},
+                        "primaries_per_s_device": n_per / ((ms_tr + ms_sg + ms_sc) / 1000.0),
+                        "primaries_per_s_wall": n_per / wall}
+        stream_ms += ms_tr + ms_sg + ms_sc
+        wall_all += wall
+    tot = len(energies) * n_per
+    return {"workload": f"{n_per} primaries at each of {', '.join(str(int(e)) for e in energies)} eV, batches of "
+                        f"{B}, box +-15 um, DNA 21 x 21 fibres, DSB window 10 bp; transport + surrogate chemistry "
+                        "+ scoring (the IRT checks 1 % of batches)",
+            "primaries_per_s_device": tot / (stream_ms / 1000.0), "primaries_per_s_wall": tot / wall_all,
+            "device_ms": stream_ms, "yields": rows}
+
+
+def run_sweep(args):
+    """DNA-damage sweep (see sweep_block) with the surrogate trained first."""
+    import wgdna
+    from wgdna import surrogate as S
+    n_per = args.np if args.np != NP else 1_000_000
+    ctx = wgdna.Context(max_primaries=4096, max_rad=8_000_000, max_sec=1_200_000)
+    train = S.train_on_irt(ctx, 8)
     with Clocks(0) as clk:
-        for E in (1000.0, 3000.0, 10000.0):
-            nb = (n_per + B - 1) // B
-            st, ssb, dsb = _lib.TransportStats(), _lib.SsbResult(), _lib.DsbResult()
-            ir = _lib.IrtResult()
-            dep = 0.0
-            n_ssb = n_dsb = 0
-            checks = []
-            Gsum = np.zeros(80)
-            ms_tr = ms_sg = ms_sc = 0.0
-            t0 = time.perf_counter()
-            for b in range(nb):
-                n = min(B, n_per - b * B)
-                p = wgdna.transport_params(n, E, box, 7.5, dna=dna, seed=int(E) * 1000 + b, dna_enable=1)
-                p.pid_base = b * B
-                _lib.check("transport", L.wgdna_transport(ctx.h, C.byref(p), C.byref(st)))
-                Gc = np.zeros(80)
-                ms = C.c_float()
-                _lib.check("chem", L.wgdna_surrogate_chemistry(ctx.h, _lib.ptr(Gc), C.byref(ms)))
-                if b % 100 == 50 or nb < 100 and b == nb // 2:                      # the IRT checks 1 %
-                    L.wgdna_irt_record_curves(ctx.h, 1)
-                    _lib.check("irt", L.wgdna_irt(ctx.h, st.n_therm, E, b + 1, C.byref(ir)))
-                    L.wgdna_irt_record_curves(ctx.h, 0)
-                    # 1 ps, 100 ps, 10 ns and 1 us are both IRT checkpoints and curve times
-                    gi = np.array(ir.G)[[0, 2, 4, 6]]
-                    gs = Gc.reshape(16, 5)[[0, 5, 10, 15]]
-                    checks.append(float((np.abs(gs - gi) / np.maximum(gi, 1e-12))[gi > 0.05].max()))
-                _lib.check("score", L.wgdna_score(ctx.h, 0x12345678, C.byref(ssb), C.byref(dsb)))
-                dep += st.dep_eV_f64
-                n_ssb += ssb.ssb
-                n_dsb += dsb.dsb
-                Gsum += Gc * n * E
-                ms_tr += st.ms_transport; ms_sg += ms.value; ms_sc += ssb.ms + dsb.ms
-            wall = time.perf_counter() - t0
-            dose = dep * 1.602e-19 / mass_kg
-            gbp = dna.n_bp * 1e-9
-            rows[int(E)] = {"primaries": n_per, "batches": nb, "dose_Gy": dose,
-                            "SSB_per_primary": n_ssb / n_per, "DSB_per_primary": n_dsb / n_per,
-                            "DSB_per_Gy_Gbp": n_dsb / (dose * gbp) if dose > 0 else 0.0,
-                            "SSB_per_Gy_Gbp": n_ssb / (dose * gbp) if dose > 0 else 0.0,
-                            "G_1us": list(np.round((Gsum / (n_per * E)).reshape(16, 5)[15], 4)),
-                            "irt_check_max_rel_err": max(checks) if checks else None, "irt_checked_batches": len(checks),
-                            "device_ms": {"transport": ms_tr, "surrogate": ms_sg, "scoring": ms_sc},
-                            "primaries_per_s_device": n_per / ((ms_tr + ms_sg + ms_sc) / 1000.0),
-                            "primaries_per_s_wall": n_per / wall}
-            stream_ms += ms_tr + ms_sg + ms_sc
-    tot = 3 * n_per
+        blk = sweep_block(ctx, n_per)
     line = {"metric": "DNA-damage sweep primaries/s (1, 3, 10 keV; transport + surrogate + scoring)",
-            "value": tot / (stream_ms / 1000.0), "unit": "primaries/s", "n_gpus": 1, "steps": 1, "warmup": 0,
-            "ms_per_step": stream_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "value": blk["primaries_per_s_device"], "unit": "primaries/s", "n_gpus": 1, "steps": 1, "warmup": 0,
+            "ms_per_step": blk["device_ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 transport / bf16-f32 surrogate", "data": "synthetic",
-            "config": {"workload": f"{n_per} primaries at each of 1, 3, 10 keV, batches of {B}, box +-15 um, "
-                                   "DNA 21 x 21 fibres, DSB window 10 bp", "training": train},
-            "yields": rows, "clocks": clk.summary()}
+            "config": {"workload": blk["workload"], "training": train},
+            "e2e": {"value": blk["primaries_per_s_wall"], "unit": "primaries/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "yields": blk["yields"], "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
     ctx.close()
 
@@ -835,6 +950,9 @@ def main():
                     help="batches in flight on one GPU (one context, stream and host thread each)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate block of the default line")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="skip the track / mixed / sweep blocks of the default line")
+    ap.add_argument("--sweep-n", type=int, default=1_000_000, help="primaries per energy of the sweep block")
     ap.add_argument("--workload", choices=["pipeline", "track", "mixed", "surrogate", "sweep"], default="pipeline",
                     help="pipeline = 4096 x 10 keV transport+IRT+scoring (the benchmark); track = one "
                          "synthetic track through the IRT; mixed = 65,536 primaries of mixed energy; "

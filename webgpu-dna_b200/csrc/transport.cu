@@ -229,28 +229,6 @@ __device__ __forceinline__ void h2ovib(const TArgs& A, Blk& b, Particle& q, floa
     }
 }
 
-// autoionisation of an excited level (primary.wgsl:473-536 and 560-619)
-__device__ __forceinline__ void autoionise(const TArgs& A, Blk& b, Particle& q, float px, float py, float pz) {
-    float3 m = gauss3(A, q, 1.1547005f);
-    float bpx = px + m.x, bpy = py + m.y, bpz = pz + m.z;
-    float eaq_s = meesungnoen_sigma(1.7f);
-    float aex = bpx, aey = bpy, aez = bpz;
-    if (eaq_s > 0.0f) {
-        float3 a = gauss3(A, q, eaq_s);
-        aex = aex + a.x; aey = aey + a.y; aez = aez + a.z;
-    }
-    float dx = aex - bpx, dy = aey - bpy, dz = aez - bpz;
-    float rsep = fmaxf(sqrtf(dx * dx + dy * dy + dz * dz), 1e-6f);
-    float prec = 1.0f - expf_(-0.711f / rsep);
-    float rr = RF();
-    if (rr < prec) {
-        h2ovib(A, b, q, bpx, bpy, bpz);
-    } else {
-        atomicAdd(&b.cnt[C_OH], 1u); atomicAdd(&b.cnt[C_EAQ], 1u); atomicAdd(&b.cnt[C_H3O], 1u);
-        put(A, b, q, bpx, bpy, bpz, 0.0f); put(A, b, q, aex, aey, aez, 1.0f); put(A, b, q, bpx, bpy, bpz, 3.0f);
-    }
-}
-
 __device__ __forceinline__ void rotate(float& dx, float& dy, float& dz, float ct, float st, float cp, float sp) {
     if (fabsf(dz) > 0.99999f) {                                  // primary.wgsl:169-170
         float sw = (dz > 0.0f) ? 1.0f : -1.0f;
@@ -322,11 +300,25 @@ struct XS {
     uint32_t vbin;
 };
 
-// the interaction after the move (primary.wgsl:180-649, secondary.wgsl:167-443)
+// Spurs of interact(): an ionisation whose e-aq thermalises nearby (code 5,
+// displaced from the ionisation site), a primary's ionisation with a tracked
+// secondary (separation estimated from the secondary's range, no e-aq entry),
+// an autoionising excitation (code 1, e-aq displaced from the displaced
+// mother site).  All three share one code path so that a warp runs it once.
+enum : int { SPUR_NONE = 0, SPUR_LOCAL = 1, SPUR_TRACKED = 2, SPUR_AUTO = 3 };
+
+// the interaction after the move (primary.wgsl:180-649, secondary.wgsl:167-443).
+// First each lane takes its branch (ionisation, excitation, vibration, DEA) up
+// to the point where it needs a spur; then the lanes that need one run it
+// together; then a primary that ionised with W_sec > cutoff emits its
+// secondary.  Every lane still draws in the reference's statement order.
 __device__ __forceinline__ void interact(const TArgs& A, Blk& b, Particle& q, Dep& dep, const XS& x) {
     const float* T = b.T;
     float E = q.E;
-    float px = q.px, py = q.py, pz = q.pz;
+    const float px = q.px, py = q.py, pz = q.pz;
+    const bool prim = q.prim;
+    int spur = SPUR_NONE;
+    float W_sec = 0.0f, bind = 0.0f;
     float r_type = RF() * x.s_tot;
     if (r_type < x.xi && E > c_SB[0]) {
         float sf[5];
@@ -342,7 +334,7 @@ __device__ __forceinline__ void interact(const TArgs& A, Blk& b, Particle& q, De
         }
         float fsum = fmaxf(sf[0] + sf[1] + sf[2] + sf[3] + sf[4], 1e-12f);
         float r_sh = RF() * fsum;
-        float bind; uint32_t shell;
+        uint32_t shell;
         if (r_sh < sf[0]) { bind = c_SB[0]; shell = 0; }
         else if (r_sh < sf[0] + sf[1]) { bind = c_SB[1]; shell = 1; }
         else if (r_sh < sf[0] + sf[1] + sf[2]) { bind = c_SB[2]; shell = 2; }
@@ -353,105 +345,19 @@ __device__ __forceinline__ void interact(const TArgs& A, Blk& b, Particle& q, De
             float Wmax = (E + bind) * 0.5f;
             float W = sample_W_sec(A, T, E, shell, r_w);
             W = fminf(fmaxf(W, bind), Wmax);
-            float W_sec = fmaxf(W - bind, 0.0f);
+            W_sec = fmaxf(W - bind, 0.0f);
             E -= W;
-            if (q.prim) {
+            if (prim) {
                 q.nion++;
                 atomicAdd(&b.cnt[D_WSUM], (uint32_t)(W * 10.0f));
                 deposit(A, dep, px, py, pz, bind);
                 if (W_sec <= A.ce) deposit(A, dep, px, py, pz, W_sec);
-                if (dna_near(A, px, py, pz) == 1u) atomicAdd(&b.cnt[C_DNA], 1u);
-                float3 m = gauss3(A, q, 1.1547005f);
-                float mpx = px + m.x, mpy = py + m.y, mpz = pz + m.z;
-                if (W_sec <= A.ce) {
-                    float eaq_s = meesungnoen_sigma(W_sec);
-                    float epx = px, epy = py, epz = pz;
-                    if (eaq_s > 0.0f) {
-                        float3 a = gauss3(A, q, eaq_s);
-                        epx = epx + a.x; epy = epy + a.y; epz = epz + a.z;
-                    }
-                    float rdx = epx - mpx, rdy = epy - mpy, rdz = epz - mpz;
-                    float r_sep = fmaxf(sqrtf(rdx * rdx + rdy * rdy + rdz * rdz), 1e-6f);
-                    float p_recomb = 1.0f - expf_(-0.711f / r_sep);
-                    float r_recomb = RF();
-                    if (r_recomb < p_recomb) {
-                        h2ovib(A, b, q, mpx, mpy, mpz);
-                    } else {
-                        atomicAdd(&b.cnt[C_OH], 1u); atomicAdd(&b.cnt[C_EAQ], 1u); atomicAdd(&b.cnt[C_H3O], 1u);
-                        put(A, b, q, mpx, mpy, mpz, 0.0f); put(A, b, q, epx, epy, epz, 5.0f); put(A, b, q, mpx, mpy, mpz, 3.0f);
-                    }
-                } else {
-                    float r_track = 0.04f * powf_(W_sec, 1.3f);
-                    float r_tail = meesungnoen_sigma(fminf(W_sec, 7.4f));
-                    float r_sep_est = fmaxf(r_track + r_tail, 1e-3f);
-                    float p_recomb_t = 1.0f - expf_(-0.711f / r_sep_est);
-                    float r_recomb_t = RF();
-                    if (r_recomb_t < p_recomb_t) {
-                        h2ovib(A, b, q, mpx, mpy, mpz);
-                    } else {
-                        atomicAdd(&b.cnt[C_OH], 1u); atomicAdd(&b.cnt[C_H3O], 1u);
-                        put(A, b, q, mpx, mpy, mpz, 0.0f); put(A, b, q, mpx, mpy, mpz, 3.0f);
-                    }
-                }
-                if (W_sec > A.ce) {                              // primary.wgsl:362-413
-                    // every emission takes a sec_buf index (counters[6]); at or
-                    // beyond max_sec the secondary is dropped together with its
-                    // angle draws and the primary's momentum update (:364)
-                    const uint32_t sec_idx = atomicAdd(&A.st->sec_tail.v, 1u);
-                    if (sec_idx < A.max_sec) {
-                        q.nsec++;
-                        float E_before = E + bind + W_sec;
-                        float cos_s;
-                        if (W_sec < 50.0f) {
-                            cos_s = 2.0f * RF() - 1.0f;
-                        } else if (W_sec <= 200.0f) {
-                            if (RF() <= 0.1f) cos_s = 2.0f * RF() - 1.0f;
-                            else cos_s = RF() * 0.70710678f;
-                        } else {
-                            float sin2 = fminf(fmaxf((1.0f - W_sec / E_before) / (1.0f + W_sec / 1022000.0f), 0.0f), 1.0f);
-                            cos_s = sqrtf(fmaxf(0.0f, 1.0f - sin2));
-                        }
-                        float sin_s = sqrtf(fmaxf(0.0f, 1.0f - cos_s * cos_s));
-                        float sps, cps;
-                        sincosf_(TWO_PI_F * RF(), &sps, &cps);
-                        float sdx = q.dx, sdy = q.dy, sdz = q.dz;
-                        rotate(sdx, sdy, sdz, cos_s, sin_s, cps, sps);
-                        float p_inc = sqrtf(E_before), p_sec = sqrtf(W_sec);
-                        float pfx = p_inc * q.dx - p_sec * sdx;
-                        float pfy = p_inc * q.dy - p_sec * sdy;
-                        float pfz = p_inc * q.dz - p_sec * sdz;
-                        float pfl = sqrtf(pfx * pfx + pfy * pfy + pfz * pfz);
-                        if (pfl > 1e-10f) { q.dx = pfx / pfl; q.dy = pfy / pfl; q.dz = pfz / pfl; }
-                        if (q.nsec >= (1u << 17)) atomicOr(&A.st->err, DERR_KEY_RANGE);
-                        StashRec r{px, py, pz, W_sec, sdx, sdy, sdz, q.pid, q.nsec};
-                        int slot = A.stash_spill ? atomicAdd(b.stn, 1) : STASH;
-                        if (slot < STASH) b.stash[slot] = r;
-                        else push_global(A, &r, 1, 0);
-                    }
-                }
-            } else {
+            } else {                                             // secondary.wgsl:192-255
                 atomicAdd(&b.cnt[SS_TERT], 1u);
                 deposit(A, dep, px, py, pz, W);
-                float3 m = gauss3(A, q, 1.1547005f);
-                float spx = px + m.x, spy = py + m.y, spz = pz + m.z;
-                float eaq_s = meesungnoen_sigma(W_sec);
-                float epx = px, epy = py, epz = pz;
-                if (eaq_s > 0.0f) {
-                    float3 a = gauss3(A, q, eaq_s);
-                    epx = epx + a.x; epy = epy + a.y; epz = epz + a.z;
-                }
-                float rdx = epx - spx, rdy = epy - spy, rdz = epz - spz;
-                float r_sep = fmaxf(sqrtf(rdx * rdx + rdy * rdy + rdz * rdz), 1e-6f);
-                float p_recomb = 1.0f - expf_(-0.711f / r_sep);
-                float r_recomb = RF();
-                if (r_recomb < p_recomb) {
-                    h2ovib(A, b, q, spx, spy, spz);
-                } else {
-                    atomicAdd(&b.cnt[C_OH], 1u); atomicAdd(&b.cnt[C_EAQ], 1u); atomicAdd(&b.cnt[C_H3O], 1u);
-                    put(A, b, q, spx, spy, spz, 0.0f); put(A, b, q, epx, epy, epz, 5.0f); put(A, b, q, spx, spy, spz, 3.0f);
-                }
-                if (dna_near(A, px, py, pz) == 1u) atomicAdd(&b.cnt[C_DNA], 1u);
             }
+            if (dna_near(A, px, py, pz) == 1u) atomicAdd(&b.cnt[C_DNA], 1u);
+            spur = (!prim || W_sec <= A.ce) ? SPUR_LOCAL : SPUR_TRACKED;
         }
     } else if (r_type < x.xi + x.xc) {
         float ef[5];
@@ -478,7 +384,7 @@ __device__ __forceinline__ void interact(const TArgs& A, Blk& b, Particle& q, De
         float d = fminf(exc_E, E);
         E -= d;
         deposit(A, dep, px, py, pz, d);
-        if (q.prim) q.nexc++;
+        if (prim) q.nexc++;
         float r_ch = RF();
         if (lvl == 0u) {
             if (r_ch < 0.65f) {
@@ -491,7 +397,7 @@ __device__ __forceinline__ void interact(const TArgs& A, Blk& b, Particle& q, De
                 atomicAdd(&b.cnt[C_OH], 2u); atomicAdd(&b.cnt[C_H2], 1u);
                 put(A, b, q, px, py, pz, 0.0f); put(A, b, q, px, py, pz, 0.0f); put(A, b, q, px, py, pz, 7.0f);
             } else if (r_ch < 0.7075f) {
-                autoionise(A, b, q, px, py, pz);
+                spur = SPUR_AUTO;                                // primary.wgsl:473-536
             } else if (r_ch < 0.961f) {
                 atomicAdd(&b.cnt[C_OH], 1u); atomicAdd(&b.cnt[C_H], 1u);
                 put(A, b, q, px, py, pz, 0.0f); put(A, b, q, px, py, pz, 2.0f);
@@ -500,7 +406,7 @@ __device__ __forceinline__ void interact(const TArgs& A, Blk& b, Particle& q, De
                 put(A, b, q, px, py, pz, 2.0f); put(A, b, q, px, py, pz, 2.0f);
             }
         } else {
-            if (r_ch < 0.50f) autoionise(A, b, q, px, py, pz);
+            if (r_ch < 0.50f) spur = SPUR_AUTO;                  // primary.wgsl:560-619
         }
         if (dna_near(A, px, py, pz) == 1u) atomicAdd(&b.cnt[C_DNA], 1u);
     } else if (r_type < x.xi + x.xc + x.svib) {
@@ -529,6 +435,80 @@ __device__ __forceinline__ void interact(const TArgs& A, Blk& b, Particle& q, De
         atomicAdd(&b.cnt[C_OH], 1u); atomicAdd(&b.cnt[C_H2], 1u);
         put(A, b, q, px, py, pz, 0.0f); put(A, b, q, px, py, pz, 6.0f); put(A, b, q, px, py, pz, 7.0f);
         E = 0.0f;
+    }
+    if (spur != SPUR_NONE) {
+        // mother (H2O+) displacement, then e-aq displacement and Onsager
+        // recombination (p = 1 - exp(-0.711 / r)) or the tracked-secondary
+        // estimate r = 0.04 W^1.3 + meesungnoen(min(W, 7.4)), then the H2Ovib
+        // channels or the OH + [e-aq] + H3O+ entries (primary.wgsl:216-353)
+        const float3 m = gauss3(A, q, 1.1547005f);
+        const float mpx = px + m.x, mpy = py + m.y, mpz = pz + m.z;
+        float epx = px, epy = py, epz = pz, p_recomb;
+        if (spur != SPUR_TRACKED) {
+            const bool au = spur == SPUR_AUTO;
+            if (au) { epx = mpx; epy = mpy; epz = mpz; }
+            const float eaq_s = meesungnoen_sigma(au ? 1.7f : W_sec);
+            if (eaq_s > 0.0f) {
+                const float3 g = gauss3(A, q, eaq_s);
+                epx = epx + g.x; epy = epy + g.y; epz = epz + g.z;
+            }
+            const float rdx = epx - mpx, rdy = epy - mpy, rdz = epz - mpz;
+            const float r_sep = fmaxf(sqrtf(rdx * rdx + rdy * rdy + rdz * rdz), 1e-6f);
+            p_recomb = 1.0f - expf_(-0.711f / r_sep);
+        } else {
+            const float r_track = 0.04f * powf_(W_sec, 1.3f);
+            const float r_tail = meesungnoen_sigma(fminf(W_sec, 7.4f));
+            const float r_sep_est = fmaxf(r_track + r_tail, 1e-3f);
+            p_recomb = 1.0f - expf_(-0.711f / r_sep_est);
+        }
+        const float r_recomb = RF();
+        if (r_recomb < p_recomb) {
+            h2ovib(A, b, q, mpx, mpy, mpz);
+        } else {
+            atomicAdd(&b.cnt[C_OH], 1u); atomicAdd(&b.cnt[C_H3O], 1u);
+            put(A, b, q, mpx, mpy, mpz, 0.0f);
+            if (spur != SPUR_TRACKED) {
+                atomicAdd(&b.cnt[C_EAQ], 1u);
+                put(A, b, q, epx, epy, epz, spur == SPUR_AUTO ? 1.0f : 5.0f);
+            }
+            put(A, b, q, mpx, mpy, mpz, 3.0f);
+        }
+    }
+    if (spur == SPUR_TRACKED) {                                  // primary.wgsl:362-413
+        // every emission takes a sec_buf index (counters[6]); at or beyond
+        // max_sec the secondary is dropped together with its angle draws and
+        // the primary's momentum update (:364)
+        const uint32_t sec_idx = atomicAdd(&A.st->sec_tail.v, 1u);
+        if (sec_idx < A.max_sec) {
+            q.nsec++;
+            float E_before = E + bind + W_sec;
+            float cos_s;
+            if (W_sec < 50.0f) {
+                cos_s = 2.0f * RF() - 1.0f;
+            } else if (W_sec <= 200.0f) {
+                if (RF() <= 0.1f) cos_s = 2.0f * RF() - 1.0f;
+                else cos_s = RF() * 0.70710678f;
+            } else {
+                float sin2 = fminf(fmaxf((1.0f - W_sec / E_before) / (1.0f + W_sec / 1022000.0f), 0.0f), 1.0f);
+                cos_s = sqrtf(fmaxf(0.0f, 1.0f - sin2));
+            }
+            float sin_s = sqrtf(fmaxf(0.0f, 1.0f - cos_s * cos_s));
+            float sps, cps;
+            sincosf_(TWO_PI_F * RF(), &sps, &cps);
+            float sdx = q.dx, sdy = q.dy, sdz = q.dz;
+            rotate(sdx, sdy, sdz, cos_s, sin_s, cps, sps);
+            float p_inc = sqrtf(E_before), p_sec = sqrtf(W_sec);
+            float pfx = p_inc * q.dx - p_sec * sdx;
+            float pfy = p_inc * q.dy - p_sec * sdy;
+            float pfz = p_inc * q.dz - p_sec * sdz;
+            float pfl = sqrtf(pfx * pfx + pfy * pfy + pfz * pfz);
+            if (pfl > 1e-10f) { q.dx = pfx / pfl; q.dy = pfy / pfl; q.dz = pfz / pfl; }
+            if (q.nsec >= (1u << 17)) atomicOr(&A.st->err, DERR_KEY_RANGE);
+            StashRec r{px, py, pz, W_sec, sdx, sdy, sdz, q.pid, q.nsec};
+            int slot = A.stash_spill ? atomicAdd(b.stn, 1) : STASH;
+            if (slot < STASH) b.stash[slot] = r;
+            else push_global(A, &r, 1, 0);
+        }
     }
     q.E = E;
 }
