@@ -26,6 +26,8 @@
 //   product idx, partner jj        philox(idx, jj, pid, 5): Box-Muller radii
 //                                  x,y,z + acceptance; philox(.., 5 | 1<<4):
 //                                  Box-Muller angles.
+#include <cstring>
+
 #include "irt.cuh"
 #include "dmath.cuh"
 
@@ -337,6 +339,7 @@ __global__ void __launch_bounds__(IB) k_irt_load(IArgs A) {
     const IrtConst& C = s_c;
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
+    const uint32_t k0 = A.key ? A.key[0] : A.k0, k1 = A.key ? A.key[1] : A.k1;
     unsigned long long n_tracks = 0, n_part = 0;
     for (;;) {
         uint32_t p = 0;
@@ -374,7 +377,7 @@ __global__ void __launch_bounds__(IB) k_irt_load(IArgs A) {
                 uint32_t blk = 0, wi = 4;
                 u4 wb = {0, 0, 0, 0};
                 auto nextd = [&]() -> double {
-                    if (wi == 4) { wb = philox(blk++, k, pid, 2u, A.k0, A.k1); wi = 0; }
+                    if (wi == 4) { wb = philox(blk++, k, pid, 2u, k0, k1); wi = 0; }
                     uint32_t a_ = wi == 0 ? wb.x : wb.z;
                     uint32_t b_ = wi == 0 ? wb.y : wb.w;
                     wi += 2;
@@ -548,6 +551,7 @@ __global__ void __launch_bounds__(IB, WG_INIT_MINB) k_irt_init(IArgs A) {
     const unsigned lt = (1u << lane) - 1u;
     const unsigned long long nitems = A.toff[A.nseg];
     const float rcut = (float)sqrt(C.r_cut2);
+    const uint32_t k0 = A.key ? A.key[0] : A.k0, k1 = A.key ? A.key[1] : A.k1;
     uint32_t* qij = s_qij[wl];
     uint32_t* qw = s_qw[wl];
     uint16_t* qk = s_qk[wl];
@@ -602,7 +606,7 @@ __global__ void __launch_bounds__(IB, WG_INIT_MINB) k_irt_init(IArgs A) {
                     need |= ok[u] && r2[u] < lo2;
                 }
                 u4 cw = {0, 0, 0, 0};
-                if (need) cw = philox_accept((j0 + kk) >> 2, i, T.pid, A.k0, A.k1);
+                if (need) cw = philox_accept((j0 + kk) >> 2, i, T.pid, k0, k1);
                 int kind[4];                            // 1: candidate, 2: near R_CUT
                 bool any = false;
 #pragma unroll
@@ -631,7 +635,7 @@ __global__ void __launch_bounds__(IB, WG_INIT_MINB) k_irt_init(IArgs A) {
                     qn += __popc(m);
                     if (qn >= 32) {
                         __syncwarp();
-                        n_pairs += init_batch(C, T, qij, qw, qk, 32, lane, A.k0, A.k1, ev_over);
+                        n_pairs += init_batch(C, T, qij, qw, qk, 32, lane, k0, k1, ev_over);
                         __syncwarp();
                         if (lane < qn - 32) { qij[lane] = qij[32 + lane]; qw[lane] = qw[32 + lane]; qk[lane] = qk[32 + lane]; }
                         qn -= 32;
@@ -642,7 +646,7 @@ __global__ void __launch_bounds__(IB, WG_INIT_MINB) k_irt_init(IArgs A) {
         }
         if (qn) {
             __syncwarp();
-            n_pairs += init_batch(C, T, qij, qw, qk, qn, lane, A.k0, A.k1, ev_over);
+            n_pairs += init_batch(C, T, qij, qw, qk, qn, lane, k0, k1, ev_over);
             __syncwarp();
         }
     }
@@ -809,6 +813,7 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
     uint32_t* pq = s_pq[wl];
     // CAP of the reference worker (:405): twice the largest track's species, plus 512
     const uint32_t capref = 2u * A.counters[3] + 512u;
+    const uint32_t k0 = A.key ? A.key[0] : A.k0, k1 = A.key ? A.key[1] : A.k1;
     for (int k = lane; k < 35; k += 32) s_tl[wl][k] = 0.0;
     int* lc = s_lc[wl];
     Heap H{s_ht[wl], s_hab[wl], A.hov_t + (size_t)gw * A.hcap, A.hov_ab + (size_t)gw * A.hcap};
@@ -943,7 +948,7 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
                 const double Di = C.D[nsp];
                 const uint32_t rowp = s_row[nsp];
                 int qn = 0;
-                const ProdCtx P{px, py, pz, tb, Di, id, pid, A.k0, A.k1};
+                const ProdCtx P{px, py, pz, tb, Di, id, pid, k0, k1};
                 const float etf = (float)et, dtm = 1e-4f + 1e-6f * etf;
                 const float rcut_hi = (float)sqrt(C.r_cut2) * 1.00001f;
                 for (int s2 = 0; s2 < 6; ++s2) {
@@ -980,7 +985,7 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
                                 const float dtb = etf - q.w + dtm;
                                 const float far = dtb > 0.0f ? sqrtf(Djf2 * dtb) * 11.8f : 0.0f;
                                 if (dlo - far > rcut_hi) goto scored;
-                                const u4 q0 = philox_pair(id, jj, pid, A.k0, A.k1);
+                                const u4 q0 = philox_pair(id, jj, pid, k0, k1);
                                 // R of r_acc for U >= uf, rounded up
                                 const float uf = __uint2float_rd(q0.w) * 2.3283064365386963e-10f;
                                 const float rhi = (fmaxf(fs, __fdividef(fsc, uf)) + fadd) * 1.00002f + 1e-6f;
@@ -999,7 +1004,7 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
                                     // second stage: the partner displaced by the same Box-Muller draws in
                                     // f32.  Per axis |g_f - g| <= 2e-3 + 2e-5 |g| (sqrt of the log near 0,
                                     // fast log and cos, 2 ulp each), sigma within [sl, sh].
-                                    const u4 q1 = philox_pair_ang(id, jj, pid, A.k0, A.k1);
+                                    const u4 q1 = philox_pair_ang(id, jj, pid, k0, k1);
                                     const float dtl = fmaxf(etf - q.w - dtm, 0.0f);
                                     const float sh = sqrtf(Djf2 * dth) * 1.00001f, sl = sqrtf(Djf2 * dtl) * 0.99999f;
                                     const float sm = 0.5f * (sh + sl), Bm = Bf + 1e-4f;
@@ -1159,6 +1164,51 @@ cudaError_t launch_irt(const IArgs& a, int device, const IrtShape& shape, cudaSt
     if (ev) cudaEventRecord(ev[2], s);
     k_irt_loop<<<blocks_for((const void*)k_irt_loop, device, shape.loop_per_sm), IB, 0, s>>>(a);
     return cudaGetLastError();
+}
+
+__global__ void k_irt_set_key(uint32_t* key, uint32_t k0, uint32_t k1) { key[0] = k0; key[1] = k1; }
+
+// The IRT launch sequence as one CUDA graph, captured on a private stream and
+// replayed on the caller's.  The seed is read from a.key (written by a
+// one-thread kernel before each replay), so one graph serves every seed; it
+// is captured again when anything else in the arguments or shapes changes.
+// If capturing fails the sequence runs as plain launches from then on.
+cudaError_t irt_graph_run(const IArgs& a, int device, const IrtShape& shape, cudaStream_t s, cudaEvent_t* ev,
+                          IrtGraph* g) {
+    if (g->off || !a.key) return launch_irt(a, device, shape, s, ev);
+    IrtGraphKey want;
+    memset(&want, 0, sizeof want);
+    want.a = a;
+    want.a.k0 = want.a.k1 = 0;
+    want.shape = shape;
+    want.device = device;
+    want.ev = ev;
+    cudaError_t e;
+    if (!g->exec || memcmp(&g->key, &want, sizeof want) != 0) {
+        if (g->exec) { cudaGraphExecDestroy(g->exec); g->exec = nullptr; }
+        cudaStream_t cs;
+        if ((e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)) != cudaSuccess) return e;
+        cudaGraph_t gr = nullptr;
+        e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            cudaError_t le = launch_irt(a, device, shape, cs, ev);
+            e = cudaStreamEndCapture(cs, &gr);
+            if (le != cudaSuccess) e = le;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&g->exec, gr, 0);
+        if (gr) cudaGraphDestroy(gr);
+        cudaStreamDestroy(cs);
+        if (e != cudaSuccess) {
+            cudaGetLastError();                  // clear the failed capture
+            g->exec = nullptr;
+            g->off = true;
+            return launch_irt(a, device, shape, s, ev);
+        }
+        g->key = want;
+    }
+    k_irt_set_key<<<1, 1, 0, s>>>(const_cast<uint32_t*>(a.key), a.k0, a.k1);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return cudaGraphLaunch(g->exec, s);
 }
 
 cudaError_t launch_group_keys(const float4* rad, unsigned long long n, unsigned long long* key, uint32_t* maxpid,

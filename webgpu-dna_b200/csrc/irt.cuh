@@ -46,6 +46,7 @@ struct IArgs {
     unsigned long long* acc;             // [0..8] rxn, 9 reacted, 10 pairs, 11 events, 12 tracks
     float* curves;                       // optional: per track 16 x 5 counts (OH, eaq, H, H2O2, H2)
     uint32_t* err;
+    const uint32_t* key;                 // optional: the Philox key (k0, k1) in device memory (graph replays)
 };
 
 cudaError_t irt_set_constants(const IrtConst& c);
@@ -56,6 +57,15 @@ struct IrtShape { uint32_t init_per_sm, loop_per_sm; };
 int irt_warps(int device, const IrtShape& shape);
 // ev (optional, 3 events): recorded after the load, the initial pairing and the sort
 cudaError_t launch_irt(const IArgs& a, int device, const IrtShape& shape, cudaStream_t s, cudaEvent_t* ev = nullptr);
+// A captured IRT launch sequence and what it was captured for (irt.cu irt_graph_run).
+struct IrtGraphKey { IArgs a; IrtShape shape; int device; cudaEvent_t* ev; };
+struct IrtGraph {
+    cudaGraphExec_t exec = nullptr;
+    IrtGraphKey key;
+    bool off = false;                    // capturing failed once: plain launches from then on
+};
+cudaError_t irt_graph_run(const IArgs& a, int device, const IrtShape& shape, cudaStream_t s, cudaEvent_t* ev,
+                          IrtGraph* g);
 cudaError_t launch_group_keys(const float4* rad, unsigned long long n, unsigned long long* key, uint32_t* maxpid,
                               cudaStream_t s);
 cudaError_t launch_seg_max(const unsigned long long* off, uint32_t nseg, unsigned long long* out, cudaStream_t s);
