@@ -396,6 +396,32 @@ def run_native(args, ws, rank, local):
         except Exception:
             traffic = None
     clocks = clk.summary()
+    # the binding resource of these kernels is issue slots (divergent Monte
+    # Carlo and f64 event chains, not bytes): warp instructions per launch (from
+    # one ncu capture, per unit processed, profiles/issue.json) / (duration x SM
+    # clock x SMs) against 4 warp instructions per cycle per SM
+    issue = None
+    isf = os.path.join(ROOT, "profiles", "issue.json")
+    if os.path.exists(isf):
+        try:
+            t = json.load(open(isf)).get(dom)
+            if t:
+                unit = {"k_transport": NPr, "k_irt_init": Np, "k_irt_loop": Np}[dom]
+                inst = t["inst_per_unit"] * unit
+                mhz = clocks.get("sm_mhz") or 1965.0
+                sms = torch.cuda.get_device_properties(dev).multi_processor_count
+                ach = inst / (kernels[dom] / 1000.0) / (mhz * 1e6) / sms
+                issue = {"achieved": ach, "peak": 4.0, "unit": "warp instructions / cycle / SM", "frac": ach / 4.0,
+                         "inst_per_launch": inst, "sm_mhz": mhz, "sms": sms, "source": "profiles/issue.json"}
+        except Exception:
+            issue = None
+    hbm = {"achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
+           "traffic": traffic, "alg_bytes": int(alg), "peak_source": "fallback" if pk.get("fallback") else "measured"}
+    if issue is not None:
+        roofline = {"bound": "issue", "kernel": dom, "achieved": issue["achieved"], "peak": issue["peak"],
+                    "unit": issue["unit"], "frac": issue["frac"], "traffic": traffic, "issue": issue, "hbm": hbm}
+    else:
+        roofline = {"bound": "hbm", "kernel": dom, **hbm}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -415,10 +441,7 @@ def run_native(args, ws, rank, local):
             "gpu_launches": launches,
             "stage_ms": {k: round(v, 4) for k, v in stages.items()},
             "kernel_ms": {k: round(v, 4) for k, v in kernels.items()},
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk["hbm_gbs"],
-                         "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
-                         "alg_bytes": int(alg),
-                         "peak_source": "fallback" if pk.get("fallback") else "measured"},
+            "roofline": roofline,
             "clocks": clocks,
             "physics": physics,
             "surrogate": surrogate,

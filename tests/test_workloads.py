@@ -66,9 +66,9 @@ def test_irt_synthetic_track_bit_exact(ctx):
 
 
 @pytest.mark.gpu
-def test_mixed_energies_transport_and_irt_bit_exact(ctx):
-    n = 192
-    E = synthetic.mixed_energies(n, key=5)
+@pytest.mark.parametrize("n,key", [(192, 5), (2048, 6)])
+def test_mixed_energies_transport_and_irt_bit_exact(ctx, n, key):
+    E = synthetic.mixed_energies(n, key=key)
     o = oracle.transport(n, 10000.0, seed=13, rng_mode=0, dna_enable=0, E_per_primary=E)
     p = wgdna.transport_params(n, 10000.0, 15000.0, 7.5, seed=13, dna_enable=0)
     Eh = np.ascontiguousarray(E, np.float32)
