@@ -444,8 +444,8 @@ extern "C" int wgdna_transport(wgdna_ctx* c, const wgdna_transport_params* p, wg
         st->dep_eV_f64 = hs.dep_f64;
         st->steps = hs.steps;
         st->n_therm = (uint32_t)red[1];
-        cudaEventElapsedTime(&st->ms_transport, c->ev[0], c->ev[1]);
-        cudaEventElapsedTime(&st->ms_canon, c->ev[2], c->ev[3]);
+        st->ms_transport = elapsed_ms(c->ev[0], c->ev[1]);
+        st->ms_canon = elapsed_ms(c->ev[2], c->ev[3]);
         st->device_error = hs.err | err2;
     }
     if (hs.err | err2) {
@@ -589,11 +589,15 @@ static int irt_run(wgdna_ctx* c, uint32_t nseg, uint32_t n_therm, double E_eV, u
         out->n_reacted = acc[9]; out->n_pairs = acc[10]; out->n_events = acc[11]; out->n_tracks = acc[12];
         out->n_particles = acc[13]; out->n_init_events = acc[14];
         out->chem_n = chem_n;
-        cudaEventElapsedTime(&out->ms, c->ev[4], c->ev[5]);
-        cudaEventElapsedTime(&out->ms_load, c->ev[4], c->ev[8]);
-        cudaEventElapsedTime(&out->ms_pairing, c->ev[8], c->ev[9]);
-        cudaEventElapsedTime(&out->ms_sort, c->ev[9], c->ev[10]);
-        cudaEventElapsedTime(&out->ms_events, c->ev[10], c->ev[5]);
+        bool timed = true;
+        out->ms = elapsed_ms(c->ev[4], c->ev[5]);
+        out->ms_load = elapsed_ms(c->ev[4], c->ev[8], &timed);
+        out->ms_pairing = elapsed_ms(c->ev[8], c->ev[9]);
+        out->ms_sort = elapsed_ms(c->ev[9], c->ev[10]);
+        out->ms_events = elapsed_ms(c->ev[10], c->ev[5]);
+        // the per-kernel events inside a replayed graph could not be timed:
+        // plain launches from the next call on, so that the times stay reported
+        if (!timed && c->irt_graph.exec) c->irt_graph.off = true;
         out->device_error = err;
     }
     if (err) { wg_set_error("wgdna_irt: device error flags 0x%x", err); return WGDNA_ERR_DEVICE; }
@@ -823,7 +827,7 @@ static int score_dev(wgdna_ctx* c, const float4* d_in, const uint32_t* d_alive, 
         unsigned long long draws = n ? u[4] : 0;
         out->in_reach = draws;
         out->lcg_state = lcg_jump_host(lcg, draws);
-        cudaEventElapsedTime(&out->ms, c->ev[6], c->ev[7]);
+        out->ms = elapsed_ms(c->ev[6], c->ev[7]);
     }
     return WGDNA_OK;
 }
@@ -882,7 +886,7 @@ static int cluster_dev(wgdna_ctx* c, wgdna_dsb_result* out) {
             out->dsb += fib[3 * f]; out->ssb0 += k0; out->ssb1 += k1;
             if (k0 > 0 && k1 > 0) out->dsb_expected += 1 - pow(1 - p_pair, (double)k0 * (double)k1);
         }
-        cudaEventElapsedTime(&out->ms, c->ev[6], c->ev[7]);
+        out->ms = elapsed_ms(c->ev[6], c->ev[7]);
     }
     return WGDNA_OK;
 }
@@ -1044,7 +1048,7 @@ extern "C" int wgdna_chem_grid(wgdna_ctx* c, const float* rad, uint64_t rad_n, u
     if (pos && cap >= n) WG_CUDA_OK(cudaMemcpyAsync(pos, c->d_cg_pos, (size_t)n * 16, cudaMemcpyDeviceToHost, s));
     if (alive && cap >= n) WG_CUDA_OK(cudaMemcpyAsync(alive, c->d_cg_alive, (size_t)n * 4, cudaMemcpyDeviceToHost, s));
     WG_CUDA_OK(cudaStreamSynchronize(s));
-    cudaEventElapsedTime(&out->ms, c->ev[4], c->ev[5]);
+    out->ms = elapsed_ms(c->ev[4], c->ev[5]);
     out->chem_n = n;
     // G per 100 eV of the deposited energy carried by the chem_n radicals (schedule.ts:218-227)
     out->deposited_eV = (double)n_therm * E_eV * ((double)n / (double)n_all);

@@ -107,6 +107,16 @@ struct DeviceOnce {
     }
 };
 
+// Elapsed time between two recorded events, or 0 when the runtime cannot
+// time them; a failed query leaves no error pending for a later launch check.
+inline float elapsed_ms(cudaEvent_t a, cudaEvent_t b, bool* ok = nullptr) {
+    float ms = 0.0f;
+    const bool good = cudaEventElapsedTime(&ms, a, b) == cudaSuccess;
+    if (!good) { cudaGetLastError(); ms = 0.0f; }
+    if (ok) *ok = good;
+    return ms;
+}
+
 }  // namespace wg
 
 #define WG_CUDA_OK(expr)                                                     \

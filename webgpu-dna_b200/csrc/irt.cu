@@ -1147,21 +1147,31 @@ int irt_warps(int device, const IrtShape& shape) {
 // tile prefix: the scan of transport.cu
 cudaError_t launch_scan_u32(const uint32_t* cnt, uint32_t n, unsigned long long* off, cudaStream_t s);
 
+// timing events of the launch sequence: inside a stream capture they must be
+// external event nodes, which a replay records like a plain cudaEventRecord
+static cudaError_t irt_mark(cudaEvent_t e, cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t r = cudaStreamIsCapturing(s, &cs);
+    if (r != cudaSuccess) return r;
+    return cudaEventRecordWithFlags(e, s, cs == cudaStreamCaptureStatusActive ? cudaEventRecordExternal
+                                                                              : cudaEventRecordDefault);
+}
+
 cudaError_t launch_irt(const IArgs& a, int device, const IrtShape& shape, cudaStream_t s, cudaEvent_t* ev) {
     { cudaError_t me_ = cudaMemsetAsync(a.counters, 0, 4 * sizeof(uint32_t), s); if (me_ != cudaSuccess) return me_; }
     k_irt_load<<<blocks_for((const void*)k_irt_load, device), IB, 0, s>>>(a);
     cudaError_t e = launch_scan_u32(a.ttiles, a.nseg, a.toff, s);
     if (e != cudaSuccess) return e;
-    if (ev) cudaEventRecord(ev[0], s);
+    if (ev && (e = irt_mark(ev[0], s)) != cudaSuccess) return e;
     k_irt_init<<<blocks_for((const void*)k_irt_init, device, shape.init_per_sm), IB, 0, s>>>(a);
-    if (ev) cudaEventRecord(ev[1], s);
+    if (ev && (e = irt_mark(ev[1], s)) != cudaSuccess) return e;
     k_track_order<<<1, 1024, 0, s>>>(a.tn, a.nseg, a.order);
     int sms = 0, per = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)k_irt_sort, SB, 0);
     const unsigned long long sgrid = (unsigned long long)sms * (unsigned long long)(per > 0 ? per : 1);
     k_irt_sort<<<(unsigned)(a.nseg < sgrid ? (a.nseg > 0 ? a.nseg : 1) : sgrid), SB, 0, s>>>(a);
-    if (ev) cudaEventRecord(ev[2], s);
+    if (ev && (e = irt_mark(ev[2], s)) != cudaSuccess) return e;
     k_irt_loop<<<blocks_for((const void*)k_irt_loop, device, shape.loop_per_sm), IB, 0, s>>>(a);
     return cudaGetLastError();
 }

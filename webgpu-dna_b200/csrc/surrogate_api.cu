@@ -407,7 +407,7 @@ extern "C" int wgdna_surrogate_chemistry(wgdna_ctx* c, double* G, float* ms) {
         cudaMemsetAsync(s->err, 0, 4, v.stream);
         return WGDNA_ERR_DEVICE;
     }
-    if (ms) cudaEventElapsedTime(ms, s->ev[0], s->ev[1]);
+    if (ms) *ms = elapsed_ms(s->ev[0], s->ev[1]);
     for (int k = 0; k < SG_OUT; ++k) G[k] = acc[SG_OUT] > 0 ? acc[k] / acc[SG_OUT] : 0.0;
     return WGDNA_OK;
 }
