@@ -112,8 +112,7 @@ struct wgdna_ctx {
     double* d_acc_tl = nullptr;
     unsigned long long* d_acc = nullptr;
     uint32_t* d_maxpid = nullptr;
-    uint32_t* d_irt_key = nullptr;        // the IRT's Philox key, read by the captured launch sequence
-    IrtGraph irt_graph;
+    IrtGraph irt_graph;                   // the IRT launch sequence, captured once per argument set
     cudaEvent_t ev[11]{};
 };
 
@@ -323,7 +322,6 @@ extern "C" void wgdna_destroy(wgdna_ctx* c) {
                     c->d_cg_prod, c->d_cg_counts, c->d_cg_head, c->d_cg_next, c->d_cg_step};
     if (c->cg_graph) cudaGraphExecDestroy(c->cg_graph);
     if (c->irt_graph.exec) cudaGraphExecDestroy(c->irt_graph.exec);
-    if (c->d_irt_key) cudaFree(c->d_irt_key);
     for (void* p : ptrs) if (p) cudaFree(p);
     for (auto& ev : c->ev) if (ev) cudaEventDestroy(ev);
     if (c->own) cudaStreamDestroy(c->own);
@@ -524,7 +522,6 @@ static int irt_ensure(wgdna_ctx* c, uint32_t nseg, uint64_t rad_n, uint32_t cap)
     if (!c->d_irt_cnt) TRY(dalloc(&c->d_irt_cnt, 4));
     if (!c->d_acc_tl) TRY(dalloc(&c->d_acc_tl, 35));
     if (!c->d_acc) TRY(dalloc(&c->d_acc, 16));
-    if (!c->d_irt_key) TRY(dalloc(&c->d_irt_key, 2));
     // the reaction constants live in __constant__ memory, which every device
     // holds separately: upload them once per device (the context's is current)
     static DeviceOnce consts;
@@ -566,7 +563,6 @@ static int irt_run(wgdna_ctx* c, uint32_t nseg, uint32_t n_therm, double E_eV, u
         c->curves_n = nseg;
     }
     WG_CUDA_OK(cudaEventRecord(c->ev[4], s));
-    a.key = c->d_irt_key;
     WG_CUDA_OK(irt_graph_run(a, c->device, IrtShape{c->tune.irt_init_blocks_per_sm, c->tune.irt_loop_blocks_per_sm},
                              s, &c->ev[8], &c->irt_graph));
     WG_CUDA_OK(cudaEventRecord(c->ev[5], s));

@@ -339,7 +339,7 @@ __global__ void __launch_bounds__(IB) k_irt_load(IArgs A) {
     const IrtConst& C = s_c;
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
-    const uint32_t k0 = A.key ? A.key[0] : A.k0, k1 = A.key ? A.key[1] : A.k1;
+    const uint32_t k0 = A.k0, k1 = A.k1;
     unsigned long long n_tracks = 0, n_part = 0;
     for (;;) {
         uint32_t p = 0;
@@ -551,7 +551,7 @@ __global__ void __launch_bounds__(IB, WG_INIT_MINB) k_irt_init(IArgs A) {
     const unsigned lt = (1u << lane) - 1u;
     const unsigned long long nitems = A.toff[A.nseg];
     const float rcut = (float)sqrt(C.r_cut2);
-    const uint32_t k0 = A.key ? A.key[0] : A.k0, k1 = A.key ? A.key[1] : A.k1;
+    const uint32_t k0 = A.k0, k1 = A.k1;
     uint32_t* qij = s_qij[wl];
     uint32_t* qw = s_qw[wl];
     uint16_t* qk = s_qk[wl];
@@ -813,7 +813,7 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
     uint32_t* pq = s_pq[wl];
     // CAP of the reference worker (:405): twice the largest track's species, plus 512
     const uint32_t capref = 2u * A.counters[3] + 512u;
-    const uint32_t k0 = A.key ? A.key[0] : A.k0, k1 = A.key ? A.key[1] : A.k1;
+    const uint32_t k0 = A.k0, k1 = A.k1;
     for (int k = lane; k < 35; k += 32) s_tl[wl][k] = 0.0;
     int* lc = s_lc[wl];
     Heap H{s_ht[wl], s_hab[wl], A.hov_t + (size_t)gw * A.hcap, A.hov_ab + (size_t)gw * A.hcap};
@@ -982,15 +982,13 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
                                 // Box-Muller radius of 32-bit draws (sqrt(3 * 2 ln 2^33) = 11.72)
                                 // times sqrt(2 D dt), and a partner beyond R_CUT after it is
                                 // rejected by the exact path too
-                                const float dtb = etf - q.w + dtm;
-                                const float far = dtb > 0.0f ? sqrtf(Djf2 * dtb) * 11.8f : 0.0f;
-                                if (dlo - far > rcut_hi) goto scored;
+                                const float dth = etf - q.w + dtm;
+                                if (dlo - (dth > 0.0f ? sqrtf(Djf2 * dth) * 11.8f : 0.0f) > rcut_hi) goto scored;
                                 const u4 q0 = philox_pair(id, jj, pid, k0, k1);
                                 // R of r_acc for U >= uf, rounded up
                                 const float uf = __uint2float_rd(q0.w) * 2.3283064365386963e-10f;
                                 const float rhi = (fmaxf(fs, __fdividef(fsc, uf)) + fadd) * 1.00002f + 1e-6f;
-                                // upper bound of dt = et - t_birth from the f32 birth time (error < dtm)
-                                const float dth = etf - q.w + dtm;
+                                // dth: upper bound of dt = et - t_birth from the f32 birth time (error < dtm)
                                 float reach = 0.0f, l0 = 0.0f, l1 = 0.0f, l2 = 0.0f, Bf = 0.0f;
                                 if (dth > 0.0f) {
                                     l0 = -2.0f * __logf((float)u01d32(q0.x));
@@ -1176,20 +1174,17 @@ cudaError_t launch_irt(const IArgs& a, int device, const IrtShape& shape, cudaSt
     return cudaGetLastError();
 }
 
-__global__ void k_irt_set_key(uint32_t* key, uint32_t k0, uint32_t k1) { key[0] = k0; key[1] = k1; }
-
 // The IRT launch sequence as one CUDA graph, captured on a private stream and
-// replayed on the caller's.  The seed is read from a.key (written by a
-// one-thread kernel before each replay), so one graph serves every seed; it
-// is captured again when anything else in the arguments or shapes changes.
-// If capturing fails the sequence runs as plain launches from then on.
+// replayed on the caller's.  It is captured again when anything in the
+// arguments (seed included) or the shapes changes; a repeated call on the same
+// tracks and seed replays it.  If capturing fails the sequence runs as plain
+// launches from then on.
 cudaError_t irt_graph_run(const IArgs& a, int device, const IrtShape& shape, cudaStream_t s, cudaEvent_t* ev,
                           IrtGraph* g) {
-    if (g->off || !a.key) return launch_irt(a, device, shape, s, ev);
+    if (g->off) return launch_irt(a, device, shape, s, ev);
     IrtGraphKey want;
     memset(&want, 0, sizeof want);
     want.a = a;
-    want.a.k0 = want.a.k1 = 0;
     want.shape = shape;
     want.device = device;
     want.ev = ev;
@@ -1216,8 +1211,6 @@ cudaError_t irt_graph_run(const IArgs& a, int device, const IrtShape& shape, cud
         }
         g->key = want;
     }
-    k_irt_set_key<<<1, 1, 0, s>>>(const_cast<uint32_t*>(a.key), a.k0, a.k1);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     return cudaGraphLaunch(g->exec, s);
 }
 

@@ -46,7 +46,6 @@ struct IArgs {
     unsigned long long* acc;             // [0..8] rxn, 9 reacted, 10 pairs, 11 events, 12 tracks
     float* curves;                       // optional: per track 16 x 5 counts (OH, eaq, H, H2O2, H2)
     uint32_t* err;
-    const uint32_t* key;                 // optional: the Philox key (k0, k1) in device memory (graph replays)
 };
 
 cudaError_t irt_set_constants(const IrtConst& c);

@@ -31,10 +31,10 @@ from . import _lib
 from .dispatch import transport_params
 from .geometry import build_dna_target
 
-TRANSPORT_CTAS = (1, 2)
-PRIM_TAKE = (1, 2, 4, 8, 32)
+TRANSPORT_CTAS = (2, 3)
+PRIM_TAKE = (1, 2, 4)
 STASH = ((16, 32), (8, 16), (4, 8), (0, 4), (0, 0), (24, 40))
-QUEUE_POLL = (1, 4, 8, 32)
+QUEUE_POLL = (4, 8, 32)
 IRT_INIT = (2, 3, 4, 5, 6)
 IRT_LOOP = (1, 2, 3, 4)
 FIELDS = ("transport_ctas_per_sm", "prim_take", "stash_keep", "stash_spill", "queue_poll",

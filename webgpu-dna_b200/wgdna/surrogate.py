@@ -88,15 +88,20 @@ def batch_G(G, E):
     return (np.asarray(G, np.float64) * w[:, None]).sum(axis=0).reshape(16, 5) / w.sum()
 
 
-def in_range(ctx, X, margin=0.0):
-    """True when every descriptor lies inside the training data's range (per
-    standardised feature, the range the model was fitted on plus a margin)."""
+def in_range(ctx, X, E=None, share=0.01, zmax=6.0):
+    """True when the batch lies inside the training data's range: the tracks
+    with a descriptor beyond zmax standard deviations of the training data
+    carry at most ``share`` of the batch's energy (of its tracks when E is
+    None).  The surrogate's batch G is an energy-weighted mean over tracks, so
+    a few rare tracks outside the range move it by at most their weight."""
     L = _lib.lib()
     nrm = np.zeros(2 * 64 + 2 * 80, np.float32)
     _lib.check("wgdna_surrogate_norm", L.wgdna_surrogate_norm(ctx.h, _lib.ptr(nrm), None))
     xm, xs = nrm[:64], nrm[64:128]
     z = (np.asarray(X) - xm) / xs
-    return bool(np.all(np.abs(z) <= 6.0 + margin))
+    out = np.any(np.abs(z) > zmax, axis=1)
+    w = np.ones(out.size) if E is None else np.asarray(E, np.float64)
+    return bool(w[out].sum() <= share * w.sum())
 
 
 def chemistry(ctx, n_therm, E_eV, seed=1):
@@ -107,7 +112,7 @@ def chemistry(ctx, n_therm, E_eV, seed=1):
     _lib.check("wgdna_track_descriptors", L.wgdna_track_descriptors(ctx.h, None, 0, C.byref(k)))
     X = np.zeros((k.value, 64), np.float32)
     _lib.check("wgdna_track_descriptors", L.wgdna_track_descriptors(ctx.h, _lib.ptr(X), k.value, C.byref(k)))
-    if in_range(ctx, X):
+    if in_range(ctx, X, np.full(k.value, E_eV)):
         G = np.zeros(80, np.float64)
         ms = C.c_float()
         _lib.check("wgdna_surrogate_chemistry", L.wgdna_surrogate_chemistry(ctx.h, _lib.ptr(G), C.byref(ms)))
