@@ -58,7 +58,7 @@ int wgdna_set_stream(wgdna_ctx *ctx, void *cuda_stream);
  * library when that file exists (written by `python -m wgdna.autotune`, one
  * "key value" line per field below), else uses the defaults shown. */
 typedef struct {
-    uint32_t transport_ctas_per_sm;  /* resident transport CTAs per SM, 0 = as many as fit (3) */
+    uint32_t transport_ctas_per_sm;  /* resident transport CTAs per SM, 0 = as many as fit (2) */
     uint32_t prim_take;              /* primaries a transport warp may start per iteration (2), 1..32 */
     uint32_t stash_keep;             /* secondaries a warp keeps when its stash spills (16) */
     uint32_t stash_spill;            /* stash level that spills to the global queue (32), <= 48;

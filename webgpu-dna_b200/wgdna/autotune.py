@@ -31,7 +31,7 @@ from . import _lib
 from .dispatch import transport_params
 from .geometry import build_dna_target
 
-TRANSPORT_CTAS = (2, 3)
+TRANSPORT_CTAS = (1, 2)
 PRIM_TAKE = (1, 2, 4)
 STASH = ((16, 32), (8, 16), (4, 8), (0, 4), (0, 0), (24, 40))
 QUEUE_POLL = (4, 8, 32)

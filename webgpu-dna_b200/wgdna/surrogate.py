@@ -88,17 +88,23 @@ def batch_G(G, E):
     return (np.asarray(G, np.float64) * w[:, None]).sum(axis=0).reshape(16, 5) / w.sum()
 
 
+# descriptors that place a track in its regime: the yields per 100 eV, log E,
+# log entries and log radius of gyration (the distance histograms and species
+# fractions are sparse and noisy per track)
+RANGE_FEATURES = slice(0, 9)
+
+
 def in_range(ctx, X, E=None, share=0.01, zmax=6.0):
     """True when the batch lies inside the training data's range: the tracks
-    with a descriptor beyond zmax standard deviations of the training data
-    carry at most ``share`` of the batch's energy (of its tracks when E is
+    with a regime descriptor beyond zmax standard deviations of the training
+    data carry at most ``share`` of the batch's energy (of its tracks when E is
     None).  The surrogate's batch G is an energy-weighted mean over tracks, so
     a few rare tracks outside the range move it by at most their weight."""
     L = _lib.lib()
     nrm = np.zeros(2 * 64 + 2 * 80, np.float32)
     _lib.check("wgdna_surrogate_norm", L.wgdna_surrogate_norm(ctx.h, _lib.ptr(nrm), None))
-    xm, xs = nrm[:64], nrm[64:128]
-    z = (np.asarray(X) - xm) / xs
+    xm, xs = nrm[:64][RANGE_FEATURES], nrm[64:128][RANGE_FEATURES]
+    z = (np.asarray(X)[:, RANGE_FEATURES] - xm) / xs
     out = np.any(np.abs(z) > zmax, axis=1)
     w = np.ones(out.size) if E is None else np.asarray(E, np.float64)
     return bool(w[out].sum() <= share * w.sum())
