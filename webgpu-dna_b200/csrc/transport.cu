@@ -304,23 +304,27 @@ struct XS {
 // displaced from the ionisation site), a primary's ionisation with a tracked
 // secondary (separation estimated from the secondary's range, no e-aq entry),
 // an autoionising excitation (code 1, e-aq displaced from the displaced
-// mother site).  All three share one code path so that a warp runs it once.
-enum : int { SPUR_NONE = 0, SPUR_LOCAL = 1, SPUR_TRACKED = 2, SPUR_AUTO = 3 };
+// mother site), and a secondary that thermalises below the cutoff (its e-aq
+// alone, code 5, secondary.wgsl:100-124).  All share one code path so that a
+// warp runs it once.
+enum : int { SPUR_NONE = 0, SPUR_LOCAL = 1, SPUR_TRACKED = 2, SPUR_AUTO = 3, SPUR_THERM = 4 };
 
 // the interaction after the move (primary.wgsl:180-649, secondary.wgsl:167-443).
 // First each lane takes its branch (ionisation, excitation, vibration, DEA) up
 // to the point where it needs a spur; then the lanes that need one run it
 // together; then a primary that ionised with W_sec > cutoff emits its
 // secondary.  Every lane still draws in the reference's statement order.
-__device__ __forceinline__ void interact(const TArgs& A, Blk& b, Particle& q, Dep& dep, const XS& x) {
+__device__ __forceinline__ void interact(const TArgs& A, Blk& b, Particle& q, Dep& dep, const XS& x, bool therm) {
     const float* T = b.T;
     float E = q.E;
     const float px = q.px, py = q.py, pz = q.pz;
     const bool prim = q.prim;
     int spur = SPUR_NONE;
     float W_sec = 0.0f, bind = 0.0f;
-    float r_type = RF() * x.s_tot;
-    if (r_type < x.xi && E > c_SB[0]) {
+    float r_type = therm ? 0.0f : RF() * x.s_tot;
+    if (therm) {
+        spur = SPUR_THERM;                                       // the lane did not move this step
+    } else if (r_type < x.xi && E > c_SB[0]) {
         float sf[5];
         if (x.grid < 0) { for (int k = 0; k < 5; ++k) sf[k] = T[S_XSF + k * XN_]; }
         else if (x.grid > 0) { for (int k = 0; k < 5; ++k) sf[k] = T[S_XSF + k * XN_ + XN_ - 1]; }
@@ -441,13 +445,16 @@ __device__ __forceinline__ void interact(const TArgs& A, Blk& b, Particle& q, De
         // recombination (p = 1 - exp(-0.711 / r)) or the tracked-secondary
         // estimate r = 0.04 W^1.3 + meesungnoen(min(W, 7.4)), then the H2Ovib
         // channels or the OH + [e-aq] + H3O+ entries (primary.wgsl:216-353)
-        const float3 m = gauss3(A, q, 1.1547005f);
-        const float mpx = px + m.x, mpy = py + m.y, mpz = pz + m.z;
-        float epx = px, epy = py, epz = pz, p_recomb;
+        float mpx = px, mpy = py, mpz = pz;
+        if (spur != SPUR_THERM) {
+            const float3 m = gauss3(A, q, 1.1547005f);
+            mpx = px + m.x; mpy = py + m.y; mpz = pz + m.z;
+        }
+        float epx = px, epy = py, epz = pz, p_recomb = 0.0f;
         if (spur != SPUR_TRACKED) {
             const bool au = spur == SPUR_AUTO;
             if (au) { epx = mpx; epy = mpy; epz = mpz; }
-            const float eaq_s = meesungnoen_sigma(au ? 1.7f : W_sec);
+            const float eaq_s = meesungnoen_sigma(au ? 1.7f : spur == SPUR_THERM ? E : W_sec);
             if (eaq_s > 0.0f) {
                 const float3 g = gauss3(A, q, eaq_s);
                 epx = epx + g.x; epy = epy + g.y; epz = epz + g.z;
@@ -461,8 +468,9 @@ __device__ __forceinline__ void interact(const TArgs& A, Blk& b, Particle& q, De
             const float r_sep_est = fmaxf(r_track + r_tail, 1e-3f);
             p_recomb = 1.0f - expf_(-0.711f / r_sep_est);
         }
-        const float r_recomb = RF();
-        if (r_recomb < p_recomb) {
+        if (spur == SPUR_THERM) {
+            put(A, b, q, epx, epy, epz, 5.0f);
+        } else if (RF() < p_recomb) {
             h2ovib(A, b, q, mpx, mpy, mpz);
         } else {
             atomicAdd(&b.cnt[C_OH], 1u); atomicAdd(&b.cnt[C_H3O], 1u);
@@ -619,24 +627,18 @@ __device__ __forceinline__ void lane_step(const TArgs& A, Blk& b, Particle& q, D
     const float box = A.box;
     const bool prim = q.prim;
     const bool out = fabsf(q.px) >= box || fabsf(q.py) >= box || fabsf(q.pz) >= box;
-    bool go = true;
+    bool go = true, therm = false;
     if (prim) {
         if (q.it >= A.ms || q.E < A.ce) { finish_primary(A, b, q, dep, 0u); go = false; }
         else if (out) { finish_primary(A, b, q, dep, 1u); go = false; }
     } else {
         if (q.it >= A.sec_steps) { q.active = false; go = false; }
         else if (q.E < A.ce) {                                   // secondary.wgsl:100-124
+            // thermalised: its e-aq is placed in interact()'s spur block
             deposit(A, dep, q.px, q.py, q.pz, q.E);
             atomicAdd(&b.cnt[C_EAQ], 1u);
-            float eaq_s = meesungnoen_sigma(q.E);
-            float epx = q.px, epy = q.py, epz = q.pz;
-            if (eaq_s > 0.0f) {
-                float3 a = gauss3(A, q, eaq_s);
-                epx = epx + a.x; epy = epy + a.y; epz = epz + a.z;
-            }
-            put(A, b, q, epx, epy, epz, 5.0f);
             atomicAdd(&b.cnt[SS_CUT], 1u);
-            q.active = false;
+            therm = true;
             go = false;
         } else if (out) {
             atomicAdd(&b.cnt[SS_BOUNDS], 1u);
@@ -667,9 +669,10 @@ __device__ __forceinline__ void lane_step(const TArgs& A, Blk& b, Particle& q, D
         }
     }
     __syncwarp(act);
-    if (go) {
-        interact(A, b, q, dep, x);
-        q.it++;
+    if (go || therm) {
+        interact(A, b, q, dep, x, therm);
+        if (go) q.it++;
+        else q.active = false;
     }
 }
 
