@@ -184,6 +184,8 @@ class Slot:
                                  max_sec=max(NPr * 250, 100_000))
         self.stream = torch.cuda.Stream(device=dev)
         self.ctx.set_stream(self.stream.cuda_stream)
+        if args.tuning:
+            self.ctx.set_tuning(**dict(kv.split("=") for kv in args.tuning.split(",")))
         self.p = wgdna.transport_params(NPr, E_EV, 15000.0, 7.5, dna=dna, seed=args.seed, dna_enable=1)
         self.p.pid_base = (rank * P + i) * NPr
         self.flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
@@ -435,7 +437,8 @@ def run_native(args, ws, rank, local):
                        "pipeline": (f"{P} batches in flight (one context, stream and host thread each; batch k on "
                                     f"slot k mod {P}); value = all batches' primaries / the span from the first "
                                     f"batch's start to the last one's end, each batch's L2 flush inside it")
-                       if P > 1 else "batches one after another"},
+                       if P > 1 else "batches one after another",
+                       **({"tuning": args.tuning} if args.tuning else {})},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": e2e_bytes["h2d"],
                     "d2h_bytes_per_step": e2e_bytes["d2h"]},
             "gpu_launches": launches,
@@ -985,6 +988,9 @@ def main():
     ap.add_argument("--np", type=int, default=NP, help="primaries per GPU per step (4096 = the benchmark)")
     ap.add_argument("--pipeline", type=int, default=1,
                     help="batches in flight on one GPU (one context, stream and host thread each)")
+    ap.add_argument("--tuning", default="",
+                    help="launch-shape overrides for every context, e.g. transport_ctas_per_sm=1,irt_loop_blocks_per_sm=2 "
+                         "(fields of wgdna_tuning; the rest from the tuning table)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate block of the default line")
     ap.add_argument("--no-workloads", action="store_true",

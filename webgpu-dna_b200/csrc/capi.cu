@@ -356,6 +356,7 @@ static IArgs make_iargs(wgdna_ctx* c, uint32_t nseg, uint64_t seed) {
     memset(&a, 0, sizeof a);
     a.rad = c->d_rad; a.seg_off = c->d_pid_off; a.nseg = nseg; a.pid_base = c->irt_pid_base;
     a.k0 = (uint32_t)seed; a.k1 = (uint32_t)(seed >> 32);
+    philox_round_keys(a.k0, a.k1, a.rk);
     a.px = c->d_px; a.py = c->d_py; a.pz = c->d_pz; a.tb = c->d_tb; a.sp = c->d_sp; a.alive = c->d_alive8;
     a.lst = c->d_lst; a.lpos = c->d_lpos;
     a.ev_t = c->d_evt; a.ev_ab = c->d_evab;

@@ -257,6 +257,21 @@ __device__ __forceinline__ u4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint
     return u4{c0, c1, c2, c3};
 }
 
+// Philox4x32-10 with its round keys supplied (rk[2r], rk[2r+1] = the key of
+// round r, as irt.cuh philox_round_keys writes them): the same function as philox()
+__device__ __forceinline__ u4 philox_rk(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, const uint32_t* rk) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+        c0 = hi1 ^ c1 ^ rk[2 * r];
+        c1 = lo1;
+        c2 = hi0 ^ c3 ^ rk[2 * r + 1];
+        c3 = lo0;
+    }
+    return u4{c0, c1, c2, c3};
+}
+
 // u32 -> [0,1] as the reference's rf(): f32(x>>1) / 2147483647.0 == f32(x>>1) * 2^-31
 __device__ __forceinline__ float u01f(uint32_t x) { return __uint2float_rn(x >> 1) * 4.65661287e-10f; }
 // two words -> double in [0,1) with 53 bits

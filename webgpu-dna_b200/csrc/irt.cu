@@ -456,8 +456,8 @@ __device__ __forceinline__ bool pair_maybe(const IrtConst& C, int ri, float r2f,
     return r2f * uf * uf <= rhs * rhs * 1.0001f;
 }
 
-__device__ __forceinline__ u4 philox_accept(uint32_t blk, uint32_t i, uint32_t pid, uint32_t k0, uint32_t k1) {
-    return philox(blk, i, pid, 3u, k0, k1);
+__device__ __forceinline__ u4 philox_accept(uint32_t blk, uint32_t i, uint32_t pid, const uint32_t* rk) {
+    return philox_rk(blk, i, pid, 3u, rk);
 }
 
 // 2) initial pairing (:539-558): one warp per (track, tile of 32 particles).
@@ -537,7 +537,7 @@ __device__ __forceinline__ uint32_t init_batch(const IrtConst& C, const InitTrac
 }
 
 #ifndef WG_INIT_MINB
-#define WG_INIT_MINB 6
+#define WG_INIT_MINB 5
 #endif
 __global__ void __launch_bounds__(IB, WG_INIT_MINB) k_irt_init(IArgs A) {
     __shared__ IrtConst s_c;
@@ -606,7 +606,7 @@ __global__ void __launch_bounds__(IB, WG_INIT_MINB) k_irt_init(IArgs A) {
                     need |= ok[u] && r2[u] < lo2;
                 }
                 u4 cw = {0, 0, 0, 0};
-                if (need) cw = philox_accept((j0 + kk) >> 2, i, T.pid, k0, k1);
+                if (need) cw = philox_accept((j0 + kk) >> 2, i, T.pid, A.rk);
                 int kind[4];                            // 1: candidate, 2: near R_CUT
                 bool any = false;
 #pragma unroll

@@ -19,10 +19,18 @@ struct IrtConst {
     double t16[16];                      // per-track curve times 10^(-3 + 0.4 k) ns
 };
 
+// the Philox4x32-10 key schedule: rk[2r], rk[2r+1] = the keys of round r
+inline void philox_round_keys(uint32_t k0, uint32_t k1, uint32_t* rk) {
+    for (int r = 0; r < 10; ++r) { rk[2 * r] = k0 + (uint32_t)r * 0x9E3779B9u; rk[2 * r + 1] = k1 + (uint32_t)r * 0xBB67AE85u; }
+}
+
 struct IArgs {
     const float4* rad;
     const unsigned long long* seg_off;   // nseg + 1
     uint32_t nseg, k0, k1, pid_base;
+    // the Philox key schedule (k0 + r W0, k1 + r W1 for rounds r = 0..9), so the
+    // pairing kernel's Philox takes its round keys from the parameter bank
+    uint32_t rk[20];
     // per-track storage (irt.cu tbase / ebase)
     double *px, *py, *pz, *tb;
     int8_t* sp;
