@@ -280,5 +280,12 @@ __device__ __forceinline__ double u01d(uint32_t a, uint32_t b) {
 }
 // one word -> double in (0,1)
 __device__ __forceinline__ double u01d32(uint32_t a) { return ((double)a + 0.5) * (1.0 / 4294967296.0); }
+// (a + 1/2) / 2^32 in f32 arithmetic (a truncating conversion and one fma):
+// at most 1.5 ulp below and 0.5 ulp above the f32 rounding of u01d32(a), the
+// same upward error as that rounding; only for the f32 bounds in front of the
+// f64 arithmetic
+__device__ __forceinline__ float u01f32(uint32_t a) {
+    return fmaf(__uint2float_rz(a), 2.3283064365386963e-10f, 1.1641532182693481e-10f);
+}
 
 }  // namespace wg

@@ -699,9 +699,9 @@ __device__ __forceinline__ bool prod_batch(const IrtConst& C, const ProdCtx& P, 
         if (dt > 0) {
             double sig = sqrt(2.0 * Dj * dt);
             // |gaussian 3-vector| <= sqrt(sum -2 ln u1_k) (Box-Muller radius), with margin
-            float l0 = -2.0f * __logf((float)u01d32(q0.x));
-            float l1 = -2.0f * __logf((float)u01d32(q0.y));
-            float l2 = -2.0f * __logf((float)u01d32(q0.z));
+            float l0 = -2.0f * __logf(u01f32(q0.x));
+            float l1 = -2.0f * __logf(u01f32(q0.y));
+            float l2 = -2.0f * __logf(u01f32(q0.z));
             double B = (double)sqrtf((l0 + l1 + l2) * 1.0001f) + 1e-4;
             double ex = pnx - xj, ey = pny - yj, ez = pnz - zj;
             double dist = sqrt(ex * ex + ey * ey + ez * ez);
@@ -991,9 +991,9 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
                                 // dth: upper bound of dt = et - t_birth from the f32 birth time (error < dtm)
                                 float reach = 0.0f, l0 = 0.0f, l1 = 0.0f, l2 = 0.0f, Bf = 0.0f;
                                 if (dth > 0.0f) {
-                                    l0 = -2.0f * __logf((float)u01d32(q0.x));
-                                    l1 = -2.0f * __logf((float)u01d32(q0.y));
-                                    l2 = -2.0f * __logf((float)u01d32(q0.z));
+                                    l0 = -2.0f * __logf(u01f32(q0.x));
+                                    l1 = -2.0f * __logf(u01f32(q0.y));
+                                    l2 = -2.0f * __logf(u01f32(q0.z));
                                     Bf = sqrtf((l0 + l1 + l2) * 1.0001f);
                                     reach = sqrtf(Djf2 * dth) * 1.00001f * (Bf + 1e-4f);
                                 }
@@ -1007,9 +1007,9 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
                                     const float sh = sqrtf(Djf2 * dth) * 1.00001f, sl = sqrtf(Djf2 * dtl) * 0.99999f;
                                     const float sm = 0.5f * (sh + sl), Bm = Bf + 1e-4f;
                                     // cos(2 pi u) = -cos(2 pi (u - 1/2)): the argument stays in [-pi, pi]
-                                    const float g0 = -sqrtf(l0) * __cosf(6.2831853f * ((float)u01d32(q1.x) - 0.5f));
-                                    const float g1 = -sqrtf(l1) * __cosf(6.2831853f * ((float)u01d32(q1.y) - 0.5f));
-                                    const float g2 = -sqrtf(l2) * __cosf(6.2831853f * ((float)u01d32(q1.z) - 0.5f));
+                                    const float g0 = -sqrtf(l0) * __cosf(6.2831853f * (u01f32(q1.x) - 0.5f));
+                                    const float g1 = -sqrtf(l1) * __cosf(6.2831853f * (u01f32(q1.y) - 0.5f));
+                                    const float g2 = -sqrtf(l2) * __cosf(6.2831853f * (u01f32(q1.z) - 0.5f));
                                     const float fx = ex - g0 * sm, fy = ey - g1 * sm, fz = ez - g2 * sm;
                                     const float d2 = sqrtf(fmaf(fz, fz, fmaf(fy, fy, fx * fx)));
                                     const float eg = 2e-3f + 2e-5f * Bm;
