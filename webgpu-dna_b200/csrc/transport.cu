@@ -72,6 +72,14 @@ struct Blk {
     int* stn;
 };
 
+// One out-of-line copy each of the step's f32 log, exp, pow and sincos: the
+// kernel is bound by instruction fetch, and a call is cheaper than another
+// inlined copy of the function at every call site.
+__device__ __noinline__ float logf_nc(float x) { return logf_pos(x); }
+__device__ __noinline__ float expf_nc(float x) { return expf_(x); }
+__device__ __noinline__ float powf_nc(float x, float y) { return powf_(x, y); }
+__device__ __noinline__ float2 sincosf_nc(float x) { float s, c; sincosf_(x, &s, &c); return make_float2(s, c); }
+
 // Out-of-line Philox block for the transport stream: the generator is drawn
 // from many call sites, and one shared copy keeps the kernel's code small
 // enough for the instruction cache.
@@ -461,12 +469,12 @@ __device__ __forceinline__ void interact(const TArgs& A, Blk& b, Particle& q, De
             }
             const float rdx = epx - mpx, rdy = epy - mpy, rdz = epz - mpz;
             const float r_sep = fmaxf(sqrtf(rdx * rdx + rdy * rdy + rdz * rdz), 1e-6f);
-            p_recomb = 1.0f - expf_(-0.711f / r_sep);
+            p_recomb = 1.0f - expf_nc(-0.711f / r_sep);
         } else {
-            const float r_track = 0.04f * powf_(W_sec, 1.3f);
+            const float r_track = 0.04f * powf_nc(W_sec, 1.3f);
             const float r_tail = meesungnoen_sigma(fminf(W_sec, 7.4f));
             const float r_sep_est = fmaxf(r_track + r_tail, 1e-3f);
-            p_recomb = 1.0f - expf_(-0.711f / r_sep_est);
+            p_recomb = 1.0f - expf_nc(-0.711f / r_sep_est);
         }
         if (spur == SPUR_THERM) {
             put(A, b, q, epx, epy, epz, 5.0f);
@@ -502,7 +510,8 @@ __device__ __forceinline__ void interact(const TArgs& A, Blk& b, Particle& q, De
             }
             float sin_s = sqrtf(fmaxf(0.0f, 1.0f - cos_s * cos_s));
             float sps, cps;
-            sincosf_(TWO_PI_F * RF(), &sps, &cps);
+            const float2 sc = sincosf_nc(TWO_PI_F * RF());
+            sps = sc.x; cps = sc.y;
             float sdx = q.dx, sdy = q.dy, sdz = q.dz;
             rotate(sdx, sdy, sdz, cos_s, sin_s, cps, sps);
             float p_inc = sqrtf(E_before), p_sec = sqrtf(W_sec);
@@ -525,7 +534,7 @@ __device__ __forceinline__ void interact(const TArgs& A, Blk& b, Particle& q, De
 __device__ __forceinline__ bool fly(const TArgs& A, Blk& b, Particle& q, XS& x, float& dist) {
     const float* T = b.T;
     float E = q.E;
-    float lE = logf_pos(E);
+    float lE = logf_nc(E);
     if (E <= T[S_XE]) { x.grid = -1; x.xi = 0.0f; x.xc = 0.0f; x.xl = T[S_XL]; x.t = 0.0f; }
     else if (E >= T[S_XE + XN_ - 1]) {
         x.grid = 1; x.xi = T[S_XI + XN_ - 1]; x.xc = T[S_XC + XN_ - 1]; x.xl = T[S_XL + XN_ - 1]; x.t = 0.0f;
@@ -560,7 +569,7 @@ __device__ __forceinline__ bool fly(const TArgs& A, Blk& b, Particle& q, XS& x, 
     x.s_tot = x.xi + x.xc + x.xl + x.svib + x.sdea;
     if (x.s_tot <= 0.0f) return false;
     float lambda = 1.0f / (NWf * x.s_tot);
-    dist = -logf_pos(fmaxf(RF(), 1e-10f)) * lambda;
+    dist = -logf_nc(fmaxf(RF(), 1e-10f)) * lambda;
     // xs_el_cos (helpers.wgsl:66-82)
     float r = RF();
     float rr = fminf(fmaxf(r, 0.0f), 1.0f);
@@ -568,7 +577,7 @@ __device__ __forceinline__ bool fly(const TArgs& A, Blk& b, Particle& q, XS& x, 
     uint32_t jlo = (uint32_t)floorf(jf);
     uint32_t jhi = jlo + 1 < NAC_ - 1 ? jlo + 1 : NAC_ - 1;
     float fj = jf - (float)jlo;
-    float lEa = (E >= T[S_XAE]) ? lE : logf_pos(T[S_XAE]);
+    float lEa = (E >= T[S_XAE]) ? lE : logf_nc(T[S_XAE]);
     float tE = (lEa - A.tab.log_xae0) * A.tab.inv_log_xae_step;
     uint32_t iE = (uint32_t)fminf(fmaxf(floorf(tE), 0.0f), (float)(NAE_ - 2));
     float fE = fminf(fmaxf(tE - (float)iE, 0.0f), 1.0f);
@@ -578,8 +587,8 @@ __device__ __forceinline__ bool fly(const TArgs& A, Blk& b, Particle& q, XS& x, 
     float cE1 = a1[jlo] + (a1[jhi] - a1[jlo]) * fj;
     float cos_el = fminf(fmaxf(cE0 + (cE1 - cE0) * fE, -1.0f), 1.0f);
     float sin_el = sqrtf(fmaxf(0.0f, 1.0f - cos_el * cos_el));
-    float sp, cp;
-    sincosf_(TWO_PI_F * RF(), &sp, &cp);
+    const float2 sc = sincosf_nc(TWO_PI_F * RF());
+    const float sp = sc.x, cp = sc.y;
     rotate(q.dx, q.dy, q.dz, cos_el, sin_el, cp, sp);
     q.px += q.dx * dist; q.py += q.dy * dist; q.pz += q.dz * dist;
     return true;
