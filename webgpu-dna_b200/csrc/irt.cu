@@ -536,6 +536,17 @@ __device__ __forceinline__ uint32_t init_batch(const IrtConst& C, const InitTrac
     return np;
 }
 
+// One out-of-line copy of the exact evaluation for the pairing kernel's two
+// call sites (measured faster than two inlined copies: less code and fewer
+// spills in the partner loop).
+struct IbOut { uint32_t np; uint32_t over; };
+__device__ __noinline__ IbOut init_batch_nc(const IrtConst& C, InitTrack T, const uint32_t* qij, const uint32_t* qw,
+                                            const uint16_t* qk, int cnt, int lane, uint32_t k0, uint32_t k1) {
+    bool over = false;
+    const uint32_t np = init_batch(C, T, qij, qw, qk, cnt, lane, k0, k1, over);
+    return IbOut{np, over ? 1u : 0u};
+}
+
 #ifndef WG_INIT_MINB
 #define WG_INIT_MINB 5
 #endif
@@ -635,7 +646,9 @@ __global__ void __launch_bounds__(IB, WG_INIT_MINB) k_irt_init(IArgs A) {
                     qn += __popc(m);
                     if (qn >= 32) {
                         __syncwarp();
-                        n_pairs += init_batch(C, T, qij, qw, qk, 32, lane, k0, k1, ev_over);
+                        const IbOut o = init_batch_nc(C, T, qij, qw, qk, 32, lane, k0, k1);
+                        n_pairs += o.np;
+                        ev_over |= o.over != 0u;
                         __syncwarp();
                         if (lane < qn - 32) { qij[lane] = qij[32 + lane]; qw[lane] = qw[32 + lane]; qk[lane] = qk[32 + lane]; }
                         qn -= 32;
@@ -646,7 +659,9 @@ __global__ void __launch_bounds__(IB, WG_INIT_MINB) k_irt_init(IArgs A) {
         }
         if (qn) {
             __syncwarp();
-            n_pairs += init_batch(C, T, qij, qw, qk, qn, lane, k0, k1, ev_over);
+            const IbOut o = init_batch_nc(C, T, qij, qw, qk, qn, lane, k0, k1);
+            n_pairs += o.np;
+            ev_over |= o.over != 0u;
             __syncwarp();
         }
     }
