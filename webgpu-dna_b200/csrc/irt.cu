@@ -633,15 +633,23 @@ __global__ void __launch_bounds__(IB, WG_INIT_MINB) k_irt_init(IArgs A) {
                     any |= kind[u] != 0;
                 }
                 if (!__any_sync(FULL, any)) continue;
+                // queue entries of the four partners, 12 bits each (kind | rr << 2 | sv << 6);
+                // the queueing loop is kept rolled (one copy of its code, fewer spills:
+                // measured faster than four unrolled copies)
+                uint64_t pk = 0;
 #pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    pk |= (uint64_t)((uint32_t)kind[u] | ((uint32_t)rr[u] << 2) | ((uint32_t)sv[u] << 6)) << (12 * u);
+#pragma unroll 1
                 for (int u = 0; u < 4; ++u) {
-                    const unsigned m = __ballot_sync(FULL, kind[u] != 0);
+                    const uint32_t f = (uint32_t)(pk >> (12 * u)) & 0xfffu;
+                    const unsigned m = __ballot_sync(FULL, (f & 3u) != 0u);
                     if (!m) continue;
-                    if (kind[u]) {
+                    if (f & 3u) {
                         const int at = qn + __popc(m & lt);
                         qij[at] = (i << 16) | (j0 + kk + u);
                         qw[at] = u == 0 ? cw.x : u == 1 ? cw.y : u == 2 ? cw.z : cw.w;
-                        qk[at] = (uint16_t)(kind[u] | (rr[u] << 2) | (si << 6) | (sv[u] << 9));
+                        qk[at] = (uint16_t)((f & 3u) | (((f >> 2) & 15u) << 2) | (si << 6) | ((f >> 6) << 9));
                     }
                     qn += __popc(m);
                     if (qn >= 32) {
