@@ -548,7 +548,7 @@ __device__ __noinline__ IbOut init_batch_nc(const IrtConst& C, InitTrack T, cons
 }
 
 #ifndef WG_INIT_MINB
-#define WG_INIT_MINB 5
+#define WG_INIT_MINB 6
 #endif
 __global__ void __launch_bounds__(IB, WG_INIT_MINB) k_irt_init(IArgs A) {
     __shared__ IrtConst s_c;
