@@ -548,7 +548,7 @@ __device__ __noinline__ IbOut init_batch_nc(const IrtConst& C, InitTrack T, cons
 }
 
 #ifndef WG_INIT_MINB
-#define WG_INIT_MINB 6
+#define WG_INIT_MINB 7
 #endif
 __global__ void __launch_bounds__(IB, WG_INIT_MINB) k_irt_init(IArgs A) {
     __shared__ IrtConst s_c;
@@ -910,6 +910,8 @@ __global__ void __launch_bounds__(IB, WG_LOOP_MINB) k_irt_loop(IArgs A) {
                     const int r = C.map[(a < b2 ? a : b2) * 6 + (a < b2 ? b2 : a)];
                     if (r < 0) continue;
                     alive[ei] = 0; alive[ej] = 0;
+                    // rolled: one copy of the list update (fewer spills in the event kernel)
+#pragma unroll 1
                     for (int w2 = 0; w2 < 2; ++w2) {
                         int k = w2 == 0 ? ei : ej, q = w2 == 0 ? a : b2;
                         uint32_t at = lpos[k];
