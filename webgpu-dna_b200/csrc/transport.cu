@@ -558,6 +558,8 @@ __device__ __forceinline__ bool fly(const TArgs& A, Blk& b, Particle& q, XS& x, 
     }
     x.sdea = 0.0f;
     if (E >= 4.0f && E <= 13.0f) {                               // xs_dea
+        // rolled: thirteen unrolled copies cost more in instruction fetch than the loop
+#pragma unroll 1
         for (int i = 0; i < 13; ++i) {
             if (E >= c_DEA_E[i] && E < c_DEA_E[i + 1]) {
                 float f = (E - c_DEA_E[i]) / (c_DEA_E[i + 1] - c_DEA_E[i]);
