@@ -192,20 +192,20 @@ struct G3 { float x, y, z; uint32_t blk, ri, b0, b1, b2, b3; };
 
 __device__ __noinline__ G3 gauss3_nc(uint32_t blk, uint32_t ri, uint32_t b0, uint32_t b1, uint32_t b2, uint32_t b3,
                                      uint32_t sub, uint32_t pid, uint32_t k0, uint32_t k1, float sigma) {
+    // four draws: words ri..3 of the current block, then (unless ri = 0) the
+    // first ri words of the next one (all four of it when ri = 4)
     G3 g;
-    g.blk = blk; g.ri = ri; g.b0 = b0; g.b1 = b1; g.b2 = b2; g.b3 = b3;
+    u4 n = {b0, b1, b2, b3};
+    if (ri != 0u) n = philox_transport(blk, sub, pid, k0, k1);
+    const uint32_t w[8] = {b0, b1, b2, b3, n.x, n.y, n.z, n.w};
     float u[4];
-    for (int k = 0; k < 4; ++k) {
-        if (g.ri == 4u) {
-            u4 o = philox_transport(g.blk, sub, pid, k0, k1);
-            g.blk++;
-            g.b0 = o.x; g.b1 = o.y; g.b2 = o.z; g.b3 = o.w;
-            g.ri = 0;
-        }
-        uint32_t v = g.ri == 0 ? g.b0 : g.ri == 1 ? g.b1 : g.ri == 2 ? g.b2 : g.b3;
-        g.ri++;
-        u[k] = u01f(v);
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+        const uint32_t v = ri == 0u ? w[d] : ri == 1u ? w[d + 1] : ri == 2u ? w[d + 2] : ri == 3u ? w[d + 3] : w[d + 4];
+        u[d] = u01f(v);
     }
+    if (ri == 0u) { g.blk = blk; g.ri = 4u; g.b0 = b0; g.b1 = b1; g.b2 = b2; g.b3 = b3; }
+    else { g.blk = blk + 1u; g.ri = ri; g.b0 = n.x; g.b1 = n.y; g.b2 = n.z; g.b3 = n.w; }
     float u1 = fmaxf(u[0], 1e-30f);
     float rr = sqrtf(-2.0f * logf_pos(u1)) * sigma;
     float sn, cs;
