@@ -35,7 +35,7 @@ TRANSPORT_CTAS = (1, 2)
 PRIM_TAKE = (1, 2, 4)
 STASH = ((16, 32), (8, 16), (4, 8), (0, 4), (0, 0), (24, 40))
 QUEUE_POLL = (4, 8, 32)
-IRT_INIT = (2, 3, 4, 5, 6)
+IRT_INIT = (4, 5, 6, 7)
 IRT_LOOP = (1, 2, 3, 4)
 FIELDS = ("transport_ctas_per_sm", "prim_take", "stash_keep", "stash_spill", "queue_poll",
           "irt_init_blocks_per_sm", "irt_loop_blocks_per_sm")
