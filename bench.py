@@ -799,19 +799,20 @@ def mixed_block(steps=2, warmup=1, seed=0):
 SURROGATE_ENERGIES = (1000.0, 3000.0, 10000.0)
 
 
-def surrogate_block(ctx, steps, warmup, train_batches=8):
+def surrogate_block(ctx, steps, warmup, train_batches=None):
     """The learned chemistry against the IRT it replaces, on held-out 4096-track
     batches at 1, 3 and 10 keV: the network is trained here, by the library's
-    own tcgen05 kernels, on ~1e5 IRT tracks (train_batches x 4096 per energy,
+    own tcgen05 kernels, on ~2e5 IRT tracks (train_batches x 4096 per energy,
     wgdna.surrogate.train_on_irt).  Per batch (wgdna.surrogate.held_out): one
-    transport, the IRT with per-track curves (the reference G(t) at the 16
-    curve times), the plain batched IRT timed on its own, and the surrogate
+    transport, the IRT with per-track curves, four runs with different seeds
+    on the same tracks (their mean is the reference G(t) at the 16 curve
+    times), the plain batched IRT timed on its own, and the surrogate
     chemistry timed on the same tracks (CUDA events of each call).  Errors: the
     largest relative error of the batch G over 5 species x 16 times (where
     G > 0.05) and at 1 us."""
     import numpy as np
     from wgdna import surrogate as S
-    train = S.train_on_irt(ctx, train_batches)
+    train = S.train_on_irt(ctx, train_batches or S.TRAIN_BATCHES)
     per_E = {}
     for E in SURROGATE_ENERGIES:
         t_irt, t_sg, e1, eall, gis, gcs = [], [], [], [], [], []
@@ -963,7 +964,7 @@ def run_sweep(args):
     from wgdna import surrogate as S
     n_per = args.np if args.np != NP else 1_000_000
     ctx = wgdna.Context(max_primaries=4096, max_rad=8_000_000, max_sec=1_200_000)
-    train = S.train_on_irt(ctx, 8)
+    train = S.train_on_irt(ctx)
     with Clocks(0) as clk:
         blk = sweep_block(ctx, n_per)
     line = {"metric": "DNA-damage sweep primaries/s (1, 3, 10 keV; transport + surrogate + scoring)",
